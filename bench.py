@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the zone crossmatch on B200.
+
+Workload (default): the 50M x 50M full-scale single pass -- A and B of 50M
+sources each, 80 % uniform over the sky + 20 % in 500 Gaussian clusters
+(sigma 0.1 deg), B = 70 % perturbed copies of A (sigma 0.3") + 30 % random,
+wrap (ra within 1" of 0/360) and polar (|dec| > 89) sources forced in,
+r = zh = 1".  Synthetic and seeded (xmatch_b200/synth.py, config1).
+
+One step = zone build of A + zone build of B + pair kernel over all of A
+against B, with the input records already resident in HBM (`value`), and
+the same through the C ABI from pinned host records to host pairs (`e2e`).
+The metric is candidate pairs per second: pairs passing the reference
+prefilter (zone band, |ddec| < r, |dra| < alpha), counted on the GPU by the
+same kernel with XM_COUNT_CAND before the timed region.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--n 50000000]
+
+Multi-GPU: the path shards by independent jobs; N ranks run N independent
+replicas (weak scaling, no collective on the data path), timed as the max
+over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ARCSEC = 1.0 / 3600.0
+METRIC = "xmatch 50Mx50M r=1\" candidate pairs/s (exact pair set)"
+UNIT = "cand-pairs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="xmatch_b200", choices=["xmatch_b200", "reference"])
+    ap.add_argument("--n", type=int, default=50_000_000, help="sources per catalog")
+    ap.add_argument("--variant", default="filter32", choices=["filter32", "plain64"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    ap.add_argument("--out", default=None, help="also append the JSON line to this file")
+    return ap.parse_args()
+
+
+def load_workload(n, seed=1001):
+    """config1 catalogs, cached per box under /tmp (generation takes ~30 s at 50M)."""
+    from xmatch_b200 import OBJ_DTYPE, synth
+    cache = "/tmp/xmatch_b200_cfg1_%d_%d" % (n, seed)
+    fa, fb = cache + "_A.bin", cache + "_B.bin"
+    if os.path.exists(fa) and os.path.exists(fb):
+        return np.fromfile(fa, OBJ_DTYPE), np.fromfile(fb, OBJ_DTYPE)
+    A, B = synth.config1(n=n, seed=seed)
+    try:
+        A.tofile(fa + ".tmp")
+        B.tofile(fb + ".tmp")
+        os.replace(fa + ".tmp", fa)
+        os.replace(fb + ".tmp", fb)
+    except OSError:
+        pass
+    return A, B
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline(A, B, r_deg, target_s, steps=1):
+    """The reference algorithm (zone-pair loop, all pairs per zone pair, per-pair
+    FP64 sincos; Worker.cu:82-123,330-366) restated in C (oracle/), on all
+    host cores, over a dec band of the same catalogs sized to ~target_s."""
+    import oracle
+    cores = os.cpu_count() or 1
+    lo = 0.0
+    width = 0.05
+    while True:
+        a = A[(A["dec"] >= lo) & (A["dec"] < lo + width)]
+        b = B[(B["dec"] >= lo - 2 * r_deg) & (B["dec"] < lo + width + 2 * r_deg)]
+        t0 = time.perf_counter()
+        p, _, st = oracle.xmatch(a, b, r_deg, mode=oracle.MODE_ALLPAIRS_SINCOS, nthreads=cores, with_dist=True)
+        dt = time.perf_counter() - t0
+        if dt * 4 >= target_s or width >= 20:
+            break
+        width = min(20.0, width * max(2.0, min(8.0, target_s / max(dt, 1e-3) / 2)))
+    times = [dt]
+    for _ in range(steps - 1):
+        t0 = time.perf_counter()
+        oracle.xmatch(a, b, r_deg, mode=oracle.MODE_ALLPAIRS_SINCOS, nthreads=cores, with_dist=True)
+        times.append(time.perf_counter() - t0)
+    t = min(times)
+    return {"value": st.n_cand / t, "unit": UNIT, "cores": cores, "kind": "port",
+            "seconds": t, "sample": "A sources with dec in [%g, %g) deg (%d) x B within +-2r (%d): %d candidate "
+            "pairs, %d matches; includes the CPU zone sort" % (lo, lo + width, len(a), len(b), st.n_cand, len(p)),
+            "matches": len(p)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    A, B = load_workload(args.n)
+    r = 1.0 * ARCSEC
+    cb = cpu_baseline(A, B, r, max(2.0, args.cpu_seconds / 4))
+    # fixed sample, W untimed + K timed steps
+    import oracle
+    lo, hi = [float(x) for x in cb["sample"].split("[")[1].split(")")[0].split(",")]
+    a = A[(A["dec"] >= lo) & (A["dec"] < hi)]
+    b = B[(B["dec"] >= lo - 2 * r) & (B["dec"] < hi + 2 * r)]
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.xmatch(a, b, r, mode=oracle.MODE_ALLPAIRS_SINCOS, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        p, _, st = oracle.xmatch(a, b, r, mode=oracle.MODE_ALLPAIRS_SINCOS, nthreads=cores)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = st.n_cand / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config1 mixture)",
+            "config": {"workload": "config1 50Mx50M r=zh=1\" (CPU sample: dec band)", "n_per_catalog": args.n,
+                       "r_arcsec": 1.0, "zh_arcsec": 1.0, "sample": cb["sample"]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference has no CPU implementation of the path; this is the oracle's restatement of "
+                    "its algorithm (zone-pair loop, all pairs per zone pair, per-pair sincos), all host threads"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import xmatch_b200 as xm
+
+    world, rank, local = dist_setup()
+    pg = False
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = True
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    A, B = load_workload(args.n)
+    n = len(A)
+    r = 1.0 * ARCSEC
+    zh = 1.0 * ARCSEC
+    flags = xm.XM_PLAIN64 if args.variant == "plain64" else xm.XM_FILTER32
+
+    ctx = xm.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    # inputs resident in HBM
+    dA = torch.from_numpy(A.view(np.uint8)).to(dev)
+    dB = torch.from_numpy(B.view(np.uint8)).to(dev)
+    torch.cuda.synchronize(dev)
+    sa = ctx.build_device(dA.data_ptr(), n, zh, 0)
+    sb = ctx.build_device(dB.data_ptr(), n, zh, 1)
+    # candidate count (metric numerator) and match count, untimed
+    _, _, st0 = ctx.match(sa, sb, r, flags | xm.XM_COUNT_CAND, fetch=False)
+    n_cand, n_match = st0["n_cand"], st0["n_match"]
+
+    def step(stats):
+        sa.rebuild_device(dA.data_ptr(), n, stats)
+        sb.rebuild_device(dB.data_ptr(), n, stats)
+        ms_ = ctx.match(sa, sb, r, flags, fetch=False)[2]
+        for k in ("ms_match", "n_tested", "n_exact", "n_border", "n_launches"):
+            setattr(stats, k, getattr(stats, k) + ms_[k])
+
+    for _ in range(args.warmup):
+        step(xm.XmStats())
+    stats = xm.XmStats()
+    if pg:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    clk = ClockSampler(local)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(stats)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    K = args.steps
+    per = {
+        "zb_count": stats.ms_zb_count / (2 * K), "zb_scan": stats.ms_zb_scan / (2 * K),
+        "zb_scatter": stats.ms_zb_scatter / (2 * K), "zb_sort_chunks": stats.ms_zb_sort / (2 * K),
+        "pair_kernel": stats.ms_match / K,
+    }
+    kept_a, kept_b = len(sa), len(sb)
+    alg_bytes = {   # algorithmic bytes per launch
+        "zb_count": 24 * n, "zb_scatter": (24 + 32) * n, "zb_sort_chunks": (32 + 40) * n,
+        "zb_scan": 8 * int(np.ceil(180 / zh)),
+        "pair_kernel": 40 * kept_a + 40 * kept_b + 24 * n_match,
+    }
+    peaks, peak_kind = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    stages = {}
+    for k, t in per.items():
+        gbs = alg_bytes[k] / (t * 1e-3) / 1e9 if t > 0 else 0.0
+        stages[k] = {"ms": t, "alg_bytes": alg_bytes[k], "GB/s": gbs, "frac": gbs / hbm}
+    dom = max(per, key=per.get)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": stages[dom]["GB/s"], "peak": hbm, "unit": "GB/s",
+                "frac": stages[dom]["frac"], "traffic": None, "peak_source": peak_kind}
+    pipeline_bytes = 64 * n * 2 + 24 * n_match
+    pipeline = {"alg_bytes": pipeline_bytes, "GB/s": pipeline_bytes / (ms * 1e-3) / 1e9,
+                "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / hbm}
+    value = world * n_cand / (ms * 1e-3)
+
+    # ---- e2e through the C ABI with host buffers ----
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 3))
+    hA = torch.empty(A.nbytes, dtype=torch.uint8, pin_memory=True)
+    hB = torch.empty(B.nbytes, dtype=torch.uint8, pin_memory=True)
+    hA.numpy()[:] = A.view(np.uint8)
+    hB.numpy()[:] = B.view(np.uint8)
+    objA = hA.numpy().view(xm.OBJ_DTYPE)
+    objB = hB.numpy().view(xm.OBJ_DTYPE)
+    cap = n_match + 1024
+    hP = torch.empty(cap * 16, dtype=torch.uint8, pin_memory=True)
+    hD = torch.empty(cap * 8, dtype=torch.uint8, pin_memory=True)
+    outP = hP.numpy().view(np.int64).reshape(-1, 2)
+    outD = hD.numpy().view(np.float64)
+
+    def e2e_step():
+        s1 = ctx.build(objA, zh, 0)
+        s2 = ctx.build(objB, zh, 1)
+        p, d, st = ctx.match(s1, s2, r, flags, out=(outP, outD))
+        s1.free()
+        s2.free()
+        return len(p)
+
+    e2e_step()
+    if pg:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    got = 0
+    for _ in range(e2e_steps):
+        got = e2e_step()
+    f1.record(stream)
+    f1.synchronize()
+    e2e_ms = f0.elapsed_time(f1) / e2e_steps
+    if pg:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    if got != n_match:
+        raise RuntimeError("e2e match count %d differs from %d" % (got, n_match))
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded config1 mixture; no survey data)",
+        "config": {"workload": "config1 50Mx50M full-scale single pass, r=zh=1\"" if n == 50_000_000 else
+                   "config1 mixture %d x %d, r=zh=1\"" % (n, n),
+                   "n_per_catalog": n, "r_arcsec": 1.0, "zh_arcsec": 1.0, "variant": args.variant,
+                   "parallelism": "replicas x%d" % world,
+                   "l2": "inputs (2 x %.1f GB records) larger than L2 (126 MB); no flush" % (24 * n / 1e9),
+                   "step": "zone build A + zone build B + pair kernel (inputs resident in HBM)"},
+        "seconds_per_step": ms * 1e-3, "candidates": n_cand, "matches": n_match,
+        "matches_per_s": world * n_match / (ms * 1e-3),
+        "tested_pairs": stats.n_tested // K, "fp64_decisions": stats.n_exact // K,
+        "border_pairs": stats.n_border // K,
+        "borderline_fraction": (stats.n_border / stats.n_tested) if stats.n_tested else 0.0,
+        "gpu_launches": int(stats.n_launches),
+        "roofline": roofline, "stages": stages, "pipeline_roofline": pipeline,
+        "clocks": clocks,
+        "e2e": {"value": world * n_cand / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 24 * n_match,
+                "path": "xm_segment_build(host) x2 + xm_match(host pairs + distances), pinned host buffers"},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(A, B, r, args.cpu_seconds)
+    sa.free()
+    sb.free()
+    ctx.close()
+    if pg:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        s = json.dumps(line)
+        print(s, flush=True)
+        if args.out:
+            with open(args.out, "a") as f:
+                f.write(s + "\n")
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,180 @@
+/*
+ * xmatch.h -- C ABI of the B200 zone crossmatch (libxmatch_b200.so).
+ *
+ * The reference (matthiaslee/Xmatch, BoostXmatch) has no plugin or FFI
+ * surface; it is one executable whose internal boundary is the Segment data
+ * contract, the Job contract and the Worker::Match / Sorter::Sort operators.
+ * Each entry point below replaces one of those; the comment names the
+ * reference interface (file:line, paths inside the BoostXmatch project).
+ *
+ * Conventions: every call returns an xm_status (XM_OK == 0), never throws,
+ * and never aborts.  Host buffers are owned by the caller.  Device data
+ * (segments, match results) is owned by the library and lives on the
+ * context's GPU.  One xm_ctx per GPU; a context is not thread-safe (use one
+ * per host thread), different contexts are independent.  Angles: degrees for
+ * inputs (as in the .idradec file), radians for the reported distance.
+ */
+#ifndef XMATCH_B200_H
+#define XMATCH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int xm_status;
+enum {
+    XM_OK = 0,
+    XM_ERR_INVALID = 1,      /* bad argument */
+    XM_ERR_CUDA = 2,         /* CUDA runtime error (see xm_last_error) */
+    XM_ERR_NOMEM = 3,        /* device or host allocation failed */
+    XM_ERR_CAPACITY = 4,     /* output buffer too small; count holds the size needed */
+    XM_ERR_MISMATCH = 5,     /* segments built with different zone heights */
+    XM_ERR_NODEVICE = 6,     /* no usable CUDA device */
+    XM_ERR_IO = 7,           /* file could not be read or written */
+    XM_ERR_BUSY = 8,         /* serving queue full / request not finished */
+    XM_ERR_TIMEOUT = 9       /* a bounded wait ran out */
+};
+
+/* One .idradec record: 24 bytes, little endian (Obj.h:21-25). */
+typedef struct xm_obj {
+    int64_t id;
+    double ra_deg;
+    double dec_deg;
+} xm_obj;
+
+typedef struct xm_ctx xm_ctx;
+typedef struct xm_segment xm_segment;
+
+/* Pair-kernel variants (xm_match flags). */
+enum {
+    XM_FILTER32 = 0,          /* default: FP32 chord^2 reject with a proven margin,
+                                 every surviving pair decided by the FP64 predicate */
+    XM_PLAIN64 = 1u << 0,     /* all-FP64: FP64 cuts, unit vectors by sincos per pair */
+    XM_COUNT_CAND = 1u << 1,  /* also count reference-prefilter candidates (stats.n_cand) */
+    XM_NO_DIST = 1u << 2      /* do not compute distances (16-byte output) */
+};
+
+/* Stats may be NULL everywhere; when given, the call accumulates into it. */
+
+/* Result buffers in HOST memory.  pairs holds (idA, idB) interleaved, i.e.
+ * exactly the 16-byte records the reference writes (Worker.cu:407-420);
+ * dist (radians, 2 asin(chord/2)) may be NULL.  If both pointers are NULL the
+ * result stays on the device and only count is returned. */
+typedef struct xm_pairs {
+    int64_t *pairs;     /* [2 * capacity] */
+    double *dist;       /* [capacity] or NULL */
+    uint64_t capacity;  /* records the arrays can hold */
+    uint64_t count;     /* out: number of matches */
+} xm_pairs;
+
+typedef struct xm_stats {
+    uint64_t n_tested;     /* pairs the pair loop evaluated */
+    uint64_t n_cand;       /* pairs passing dec + RA cuts (XM_COUNT_CAND) */
+    uint64_t n_border;     /* FP32 value inside the margin band */
+    uint64_t n_exact;      /* pairs decided by the FP64 predicate */
+    uint64_t n_match;
+    uint64_t n_tiles;
+    uint32_t n_launches;   /* kernels launched by the call */
+    uint32_t n_retries;    /* output-buffer growth re-runs */
+    float ms_total;        /* device time of the call (CUDA events) */
+    float ms_match;        /* device time of the pair kernel alone */
+    float ms_build;        /* zone build (xm_segment_build*) */
+    float ms_h2d, ms_d2h;
+    /* zone-build passes: histogram, scan, scatter into zones, sort + SoA write */
+    float ms_zb_count, ms_zb_scan, ms_zb_scatter, ms_zb_sort;
+} xm_stats;
+
+/* Tuning of the persistent pair kernel (0 = default / autotuned). */
+typedef struct xm_tuning {
+    uint32_t tile;        /* A objects per tile (= threads per block): 64, 128, 256 */
+    uint32_t chunk;       /* tiles claimed per work-stealing step */
+    uint32_t blocks_per_sm;
+} xm_tuning;
+
+/* ---- context (replaces CudaManager / CudaContext, CudaManager.cpp:8-65) ---- */
+xm_status xm_ctx_create(int device, xm_ctx **out);
+xm_status xm_ctx_destroy(xm_ctx *ctx);
+const char *xm_status_str(xm_status s);
+const char *xm_last_error(const xm_ctx *ctx);
+/* Library and device description, e.g. for logs. */
+xm_status xm_ctx_info(const xm_ctx *ctx, int *device, int *sm_count, uint64_t *free_bytes,
+                      uint64_t *total_bytes);
+xm_status xm_ctx_synchronize(xm_ctx *ctx);
+/* The cudaStream_t all work of this context is queued on (for callers that
+ * time or order their own work against the library's). */
+xm_status xm_ctx_stream(const xm_ctx *ctx, void **stream);
+
+/* ---- zone builder (replaces Sorter::Sort, Sorter.cu:141-185) ----
+ * Assigns dec zones of height zh_deg, sorts each zone by ra on the GPU and
+ * keeps the sorted SoA (id, ra/dec radians, FP32 unit vector) resident.
+ * Objects whose zone is outside [0, ceil(180/zh)) are dropped, except
+ * dec = +90 which is kept in the last zone.  seg_id mirrors Segment::mId. */
+xm_status xm_segment_build(xm_ctx *ctx, uint32_t seg_id, const xm_obj *host_objs,
+                           uint64_t n, double zh_deg, xm_segment **out, xm_stats *stats);
+/* Same, from records already in this context's device memory. */
+xm_status xm_segment_build_device(xm_ctx *ctx, uint32_t seg_id, const xm_obj *dev_objs,
+                                  uint64_t n, double zh_deg, xm_segment **out, xm_stats *stats);
+/* Re-use seg's device storage for new records (no allocation if they fit). */
+xm_status xm_segment_rebuild_device(xm_segment *seg, const xm_obj *dev_objs, uint64_t n,
+                                    xm_stats *stats);
+xm_status xm_segment_free(xm_segment *seg);
+/* Segment fields (Segment.h:24-26): kept objects, zone count, zone height. */
+xm_status xm_segment_info(const xm_segment *seg, uint32_t *seg_id, uint64_t *n_kept,
+                          int32_t *n_zones, double *zh_deg);
+/* Copy the sorted segment to the host, as Sorter.cu:178-182 fills
+ * Segment::vId, vRadec, vZoneBegin, vZoneEnd.  Any pointer may be NULL.
+ * radec: [2*n_kept] radians; zone_begin/zone_end: [n_zones]. */
+xm_status xm_segment_export(const xm_segment *seg, int64_t *id, double *radec,
+                            int32_t *zone_begin, int32_t *zone_end);
+
+/* ---- match one job (replaces Worker::Match, Worker.cu:243-428, and the
+ * kernel xmatch_kernel, Worker.cu:65-241) ----
+ * Finds every (a in A, b in B) with b's zone within ceil(r/zh) zones of a's,
+ * |dec_a - dec_b| < r, |ra_a - ra_b| (mod 2 pi branches) < alpha(zone_a) and
+ * chord^2 < (2 sin(r/2))^2, all in FP64, each pair once, self-pairs kept. */
+xm_status xm_match(xm_ctx *ctx, const xm_segment *A, const xm_segment *B, double sr_deg,
+                   uint32_t flags, xm_pairs *out, xm_stats *stats);
+/* Copy the device-resident result of the last xm_match / xm_match_batch of
+ * this context to the host (first `out->capacity` records). */
+xm_status xm_fetch_pairs(xm_ctx *ctx, xm_pairs *out);
+
+/* ---- many jobs in one persistent launch (replaces JobManager + the worker
+ * threads, JobManager.cpp:5-47, Worker.cu:430-485) ---- */
+typedef struct xm_job {
+    const xm_segment *A;
+    const xm_segment *B;
+    double sr_deg;
+} xm_job;
+/* outs[j] receives job j's pairs (host); job_counts[j] its count.  With
+ * outs == NULL the results stay on the device, grouped by job. */
+xm_status xm_match_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags,
+                         const xm_tuning *tuning, xm_pairs *outs, uint64_t *job_counts,
+                         xm_stats *stats);
+/* Times a few tile/chunk settings on the batch and returns the fastest. */
+xm_status xm_autotune_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags,
+                            xm_tuning *best, float *best_ms, float *fixed_ms);
+
+/* ---- formats (Segment::Load, Segment.cpp:14-22; output, Worker.cu:407-420) ---- */
+/* Number of 24-byte records in a .idradec file. */
+xm_status xm_idradec_count(const char *path, uint64_t *n);
+/* Read records [first, first + n) of a .idradec file into host memory. */
+xm_status xm_idradec_read(const char *path, uint64_t first, uint64_t n, xm_obj *out);
+xm_status xm_idradec_write(const char *path, const xm_obj *objs, uint64_t n);
+/* Append pairs to a file: mode 16 = reference records {idA, idB};
+ * mode 24 = {idA, idB, dist}; mode 0 = ASCII "idA idB dist\n". */
+xm_status xm_pairs_write(const char *path, const xm_pairs *pairs, int mode, int append);
+
+/* ---- utilities ---- */
+/* FP64 unit vectors of (ra, dec) in degrees computed on the GPU exactly as
+ * the zone builder does (xyz: [3*n] host). */
+xm_status xm_unit_vectors(xm_ctx *ctx, const double *ra_deg, const double *dec_deg, uint64_t n,
+                          double *xyz);
+/* RA half-width of Common.cu:17-23 for every zone, as the library uses it. */
+xm_status xm_alpha_table(double sr_deg, double zh_deg, double *alpha, int32_t n_zones);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XMATCH_B200_H */

@@ -1,0 +1,234 @@
+"""GPU parity: every result of the CUDA path (through the C ABI) against the
+oracle on the same inputs.  Pair sets and sorted segments must be
+bit-identical; distances within 1e-12 rad."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import OBJ_DTYPE
+
+pytestmark = pytest.mark.gpu
+
+ARCSEC = 1.0 / 3600.0
+DIST_TOL = 1e-12   # radians
+
+
+def sp(p, d=None):
+    o = np.lexsort((p[:, 1], p[:, 0]))
+    return (p[o], d[o]) if d is not None else p[o]
+
+
+def objs(ids, ra, dec):
+    o = np.empty(len(ids), OBJ_DTYPE)
+    o["id"], o["ra"], o["dec"] = ids, ra, dec
+    return o
+
+
+def run_gpu(ctx, A, B, r_arcsec, zh_arcsec=None, flags=0, tuning=None):
+    import xmatch_b200 as xm
+    zh = (zh_arcsec or r_arcsec) * ARCSEC
+    sa = ctx.build(A, zh, 0)
+    sb = ctx.build(B, zh, 1)
+    if tuning is None:
+        p, d, st = ctx.match(sa, sb, r_arcsec * ARCSEC, flags | xm.XM_COUNT_CAND)
+    else:
+        res, cnt, st = ctx.match_batch([(sa, sb, r_arcsec * ARCSEC)], flags | xm.XM_COUNT_CAND, tuning=tuning)
+        p, d = res[0]
+    sa.free()
+    sb.free()
+    return p, d, st
+
+
+def check_parity(ctx, A, B, r_arcsec, zh_arcsec=None, variants=(0, 1), tuning=None):
+    po, do, so = oracle.xmatch(A, B, r_arcsec * ARCSEC, (zh_arcsec or r_arcsec) * ARCSEC)
+    po, do = sp(po, do)
+    for flags in variants:
+        p, d, st = run_gpu(ctx, A, B, r_arcsec, zh_arcsec, flags, tuning)
+        p, d = sp(p, d)
+        assert len(p) == len(po), (flags, len(p), len(po))
+        assert np.array_equal(p, po), flags
+        assert np.max(np.abs(d - do), initial=0) <= DIST_TOL
+        assert st["n_cand"] == so.n_cand, (flags, st["n_cand"], so.n_cand)
+        assert st["n_match"] == len(po)
+    return po, so
+
+
+def test_unit_vectors_bit_exact(ctx):
+    rng = np.random.default_rng(11)
+    ra = np.concatenate([rng.uniform(0, 360, 100_000), [0.0, -0.0, 90.0, 180.0, 270.0, 359.9999999, 1e-300]])
+    dec = np.concatenate([rng.uniform(-90, 90, 100_000), [0.0, 0.0, 90.0, -90.0, 45.0, -1e-12, 0.0]])
+    g = ctx.unit_vectors(ra, dec)
+    o = oracle.unit_vectors(ra, dec)
+    assert g.tobytes() == o.tobytes()
+
+
+@pytest.mark.parametrize("zh_arcsec", [1, 5, 30])
+def test_segment_build_matches_oracle(ctx, fixtures, zh_arcsec):
+    a, _ = fixtures
+    seg = ctx.build(a, zh_arcsec * ARCSEC)
+    ids, radec, zb, ze = seg.export()
+    oid, ordec, ozb, oze = oracle.build_export(a, zh_arcsec * ARCSEC)
+    assert np.array_equal(ids, oid)
+    assert radec.tobytes() == ordec.tobytes()
+    assert np.array_equal(zb, ozb) and np.array_equal(ze, oze)
+    seg.free()
+
+
+@pytest.mark.parametrize("r", [1, 5, 30])
+def test_fixture_self_match(ctx, fixtures, golden_dir, r):
+    a, _ = fixtures
+    po, _ = check_parity(ctx, a, a, r)
+    f = os.path.join(golden_dir, "pairs_test_x_test_r%d.npz" % r)
+    if os.path.exists(f):
+        assert np.array_equal(po, np.load(f)["pairs"])
+
+
+@pytest.mark.parametrize("r", [1, 5, 30])
+def test_fixture_cross_match(ctx, fixtures, r):
+    a, a2 = fixtures
+    check_parity(ctx, a2, a, r)
+    check_parity(ctx, a, a2, r)
+
+
+def test_config0_shape_small(ctx):
+    from xmatch_b200 import synth
+    A, B = synth.config0(n_a=50_000, n_b=50_000, seed=5)
+    check_parity(ctx, A, B, 3)
+
+
+def test_wrap_and_pole_dense(ctx):
+    rng = np.random.default_rng(12)
+    n = 20_000
+    ra = np.concatenate([rng.uniform(0, 0.01, n), rng.uniform(359.99, 360, n), rng.uniform(0, 360, n)])
+    ra = np.where(ra >= 360, 0.0, ra)
+    dec = np.concatenate([rng.uniform(-1, 1, 2 * n), rng.uniform(89.9, 90.0, n)])
+    A = objs(np.arange(3 * n), ra, dec)
+    B = objs(np.arange(3 * n) + 10 ** 9, (ra + rng.normal(0, 1e-4, 3 * n)) % 360.0,
+             np.clip(dec + rng.normal(0, 1e-4, 3 * n), -90, 90))
+    for r in (1, 10):
+        check_parity(ctx, A, B, r)
+
+
+def test_south_pole_and_full_ring_zones(ctx):
+    rng = np.random.default_rng(13)
+    n = 5000
+    A = objs(np.arange(n), rng.uniform(0, 360, n), -90 + rng.uniform(0, 0.02, n))
+    B = objs(np.arange(n) + 10 ** 6, rng.uniform(0, 360, n), -90 + rng.uniform(0, 0.02, n))
+    check_parity(ctx, A, B, 20)
+
+
+def test_zone_height_differs_from_radius(ctx, fixtures):
+    a, a2 = fixtures
+    check_parity(ctx, a2, a, 5, zh_arcsec=2)      # nz = 3
+    check_parity(ctx, a2, a, 5, zh_arcsec=7.5)    # nz = 1, zones taller than r
+
+
+def test_oversize_zones(ctx):
+    # every source in one 10" zone: zones far larger than the shared-memory sort chunk
+    rng = np.random.default_rng(14)
+    n = 30_000
+    A = objs(np.arange(n), rng.uniform(0, 2, n), rng.uniform(0, 0.0027, n))
+    B = objs(np.arange(n) + 10 ** 6, rng.uniform(0, 2, n), rng.uniform(0, 0.0027, n))
+    check_parity(ctx, A, B, 10, variants=(0,))
+    seg = ctx.build(A, 10 * ARCSEC)
+    ids, radec, zb, ze = seg.export()
+    oid, ordec, ozb, oze = oracle.build_export(A, 10 * ARCSEC)
+    assert np.array_equal(ids, oid) and radec.tobytes() == ordec.tobytes()
+    seg.free()
+
+
+def test_empty_single_and_dropped(ctx):
+    E = np.empty(0, OBJ_DTYPE)
+    one = objs([7], [10.0], [10.0])
+    bad = objs([1, 2, 3, 4, 5], [0.0, 0.0, np.nan, 5.0, np.inf], [90.0, 91.0, 0.0, np.nan, 1.0])
+    north = objs([9], [200.0], [90.0])
+    for x, y in ((E, E), (E, one), (one, E), (one, one), (bad, north), (bad, bad)):
+        check_parity(ctx, x, y, 1)
+
+
+def test_duplicate_coordinates(ctx):
+    # identical (ra, dec) for many ids: ties in the sort key, zero distances
+    n = 3000
+    A = objs(np.arange(n), np.full(n, 123.456), np.full(n, -33.3))
+    check_parity(ctx, A, A, 1, variants=(0,))
+
+
+@pytest.mark.parametrize("tile,chunk", [(64, 1), (128, 4), (256, 16)])
+def test_tuning_does_not_change_results(ctx, fixtures, tile, chunk):
+    a, _ = fixtures
+    check_parity(ctx, a, a, 5, variants=(0,), tuning=(tile, chunk, 0))
+
+
+def test_output_growth_never_truncates(ctx):
+    # 2,500 sources inside 20": every pair matches at r = 60" (6.25 M pairs,
+    # far beyond the initial 2 * max(nA, nB) buffer)
+    rng = np.random.default_rng(15)
+    n = 2500
+    A = objs(np.arange(n), 100 + rng.uniform(0, 20 * ARCSEC, n), 20 + rng.uniform(0, 20 * ARCSEC, n))
+    p, d, st = run_gpu(ctx, A, A, 60)
+    assert len(p) == n * n
+    assert st["n_retries"] >= 1
+    po, do, _ = oracle.xmatch(A, A, 60 * ARCSEC)
+    assert np.array_equal(sp(p), sp(po))
+
+
+def test_capacity_error_reports_count(ctx, fixtures):
+    import ctypes
+    import xmatch_b200 as xm
+    a, _ = fixtures
+    sa = ctx.build(a, 5 * ARCSEC)
+    small = np.empty((10, 2), np.int64)
+    p = xm.XmPairs(small.ctypes.data, None, 10, 0)
+    rc = xm._lib.xm_match(ctx._h, sa.handle, sa.handle, 5 * ARCSEC, 0, ctypes.byref(p), None)
+    assert rc == xm._capi.XM_ERR_CAPACITY and p.count == 10980
+    pairs, dist = ctx.fetch(p.count)     # the result is still on the device
+    assert len(pairs) == 10980
+    sa.free()
+
+
+def test_mismatched_zone_heights_rejected(ctx, fixtures):
+    import xmatch_b200 as xm
+    a, _ = fixtures
+    s1 = ctx.build(a, 1 * ARCSEC)
+    s2 = ctx.build(a, 2 * ARCSEC)
+    with pytest.raises(xm.XmatchError) as e:
+        ctx.match(s1, s2, ARCSEC)
+    assert e.value.status == xm._capi.XM_ERR_MISMATCH
+    s1.free()
+    s2.free()
+
+
+def test_batch_equals_single_jobs(ctx, fixtures):
+    from xmatch_b200 import synth
+    jobs = synth.config2_jobs(n_jobs=12, seed=3, scale=0.1)
+    segs = []
+    for A, B, r in jobs:
+        zh = r * ARCSEC
+        segs.append((ctx.build(A, zh), ctx.build(B, zh), r * ARCSEC))
+    res, cnt, st = ctx.match_batch(segs)
+    for k, (A, B, r) in enumerate(jobs):
+        po, do, _ = oracle.xmatch(A, B, r * ARCSEC)
+        p, d = res[k]
+        assert cnt[k] == len(po)
+        p, d = sp(p, d)
+        po, do = sp(po, do)
+        assert np.array_equal(p, po)
+        assert np.max(np.abs(d - do), initial=0) <= DIST_TOL
+    for a, b, _ in segs:
+        a.free()
+        b.free()
+
+
+def test_segmentation_invariance(ctx, fixtures):
+    a, _ = fixtures
+    whole, _, _ = oracle.xmatch(a, a, 5 * ARCSEC)
+    zh = 5 * ARCSEC
+    segs = [ctx.build(a[s:s + 2020], zh, k) for k, s in enumerate(range(0, len(a), 2020))]
+    jobs = [(x, y, 5 * ARCSEC) for x in segs for y in segs]
+    res, cnt, _ = ctx.match_batch(jobs)
+    allp = np.concatenate([r[0] for r in res])
+    assert np.array_equal(sp(allp), sp(whole))
+    for s in segs:
+        s.free()

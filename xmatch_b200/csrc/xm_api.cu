@@ -1,0 +1,654 @@
+// xm_api.cu -- C ABI of libxmatch_b200: contexts, segments, match calls.
+//
+// Host-side counterpart of the reference's Worker::Match (Worker.cu:243-428)
+// and Sorter::Sort (Sorter.cu:141-185): parameters and the per-zone RA
+// half-width are computed here with the host libm exactly as the reference
+// host code does (Worker.cu:310-317, 349; Common.cu:7-23), the device work is
+// queued on the context's stream, and results are copied back only when the
+// caller asks for them.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "xm_internal.h"
+#include "xm_match.cuh"
+#include "xm_math.cuh"
+
+// ---------------------------------------------------------------------------
+// RA half-width per zone, Gray, Nieto & Szalay (2007) as written in
+// Common.cu:7-23 (including its parenthesisation atan(sin t) / sqrt(...),
+// which is never smaller than the exact half-width).  Host libm on purpose:
+// the reference evaluates it on the host (Worker.cu:349).
+// ---------------------------------------------------------------------------
+static double calc_alpha_dec(double theta, double abs_dec)
+{
+    if (abs_dec + theta > 89.99) return 180;
+    return std::fabs(std::atan(std::sin(theta / XM_RAD2DEG)) /
+                     std::sqrt(std::fabs(std::cos((abs_dec - theta) / XM_RAD2DEG) *
+                                         std::cos((abs_dec + theta) / XM_RAD2DEG))));
+}
+
+static double calc_alpha_zone(double theta, double zh_deg, int zone)
+{
+    double dec = std::fabs(zone * zh_deg - 90);
+    double dec2 = std::fabs((zone + 1) * zh_deg - 90);
+    dec = (dec > dec2 ? dec : dec2);
+    return calc_alpha_dec(theta, dec + 0.01 * theta);
+}
+
+void xm_host_alpha_table(double sr_deg, double zh_deg, int32_t n_zones, double *out)
+{
+    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (n_zones < 65536) nt = 1;
+    auto work = [&](unsigned t) {
+        int64_t a = (int64_t)n_zones * t / nt, b = (int64_t)n_zones * (t + 1) / nt;
+        for (int64_t z = a; z < b; ++z) out[z] = calc_alpha_zone(sr_deg, zh_deg, (int)z);
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
+}
+
+static int32_t zones_for(double zh_deg) { return (int32_t)std::ceil(180 / zh_deg); }   // Sorter.cu:156
+
+static float round_up_f(double v)
+{
+    float f = (float)v;
+    if ((double)f < v) f = std::nextafter(f, INFINITY);
+    return f;
+}
+
+static float round_down_f(double v)
+{
+    float f = (float)v;
+    if ((double)f > v) f = std::nextafter(f, -INFINITY);
+    return f;
+}
+
+// Worker.cu:310-317 plus the FP32 margin bounds.
+//
+// With X the FP64 unit vectors and X~ = fl32(X): |X~_i - X_i| <= 2^-25, so the
+// exact differences satisfy ||D~ - D|| <= delta = sqrt(3) 2^-24.  If the FP64
+// chord^2 is below T then ||D|| < sqrt(T)(1 + 8u64) = R, and the FP32 value,
+// with one rounding of each difference and three in the fused sum of squares,
+// is at most H = ((R + delta)(1 + u32))^2 (1 + u32)^3.  A pair whose FP32
+// value exceeds H therefore cannot match; thr_lo is the mirror bound below
+// which the FP64 value is certainly under T (used for statistics only).
+xm_status xm_make_params(double sr_deg, double zh_deg, xm_match_params *p)
+{
+    if (!(sr_deg > 0) || !(zh_deg > 0) || !std::isfinite(sr_deg) || !std::isfinite(zh_deg)) return XM_ERR_INVALID;
+    p->sr_deg = sr_deg;
+    p->nz = (int32_t)std::ceil(sr_deg / zh_deg);
+    p->sr_rad = sr_deg / XM_RAD2DEG;
+    double d = 2.0 * std::sin(p->sr_rad / 2.0);
+    p->sr_dist2 = d * d;
+    const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
+    const double delta = std::sqrt(3.0) * std::ldexp(1.0, -24) * (1 + 1e-6);
+    const double rt = std::sqrt(p->sr_dist2);
+    double R = rt * (1 + 8 * u64);
+    double H = (R + delta) * (1 + u32);
+    H = H * H * std::pow(1 + u32, 3) * (1 + 1e-6);
+    p->thr_hi = round_up_f(H);
+    double Rl = rt * (1 - 8 * u64) - delta;
+    double L = 0;
+    if (Rl > 0) {
+        L = Rl * (1 - u32);
+        L = L * L * std::pow(1 - u32, 3) * (1 - 1e-6);
+    }
+    p->thr_lo = round_down_f(L);
+    return XM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+xm_status xm_dev_alloc(xm_ctx *ctx, void **p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->last_error = std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
+                          cudaGetErrorString(e);
+        *p = nullptr;
+        return XM_ERR_NOMEM;
+    }
+    return XM_OK;
+}
+
+void xm_dev_free(xm_ctx *ctx, void *p)
+{
+    if (p) cudaFreeAsync(p, ctx->stream);
+}
+
+extern "C" const char *xm_status_str(xm_status s)
+{
+    switch (s) {
+    case XM_OK: return "ok";
+    case XM_ERR_INVALID: return "invalid argument";
+    case XM_ERR_CUDA: return "CUDA error";
+    case XM_ERR_NOMEM: return "out of memory";
+    case XM_ERR_CAPACITY: return "output buffer too small";
+    case XM_ERR_MISMATCH: return "segments have different zone heights";
+    case XM_ERR_NODEVICE: return "no CUDA device";
+    case XM_ERR_IO: return "I/O error";
+    case XM_ERR_BUSY: return "busy";
+    case XM_ERR_TIMEOUT: return "timed out";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char *xm_last_error(const xm_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+extern "C" xm_status xm_ctx_create(int device, xm_ctx **out)
+{
+    if (!out) return XM_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return XM_ERR_NODEVICE;
+    }
+    if (device < 0 || device >= n) return XM_ERR_INVALID;
+    xm_ctx *ctx = new xm_ctx();
+    ctx->device = device;
+    auto fail = [&](cudaError_t e) {
+        ctx->last_error = cudaGetErrorString(e);
+        delete ctx;
+        return XM_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return fail(e);
+    if ((e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+        return fail(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if ((e = cudaMemPoolCreate(&ctx->pool, &props)) != cudaSuccess) return fail(e);
+    uint64_t thr = UINT64_MAX;   // keep freed blocks for reuse by this context
+    cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    for (auto &ev : ctx->ev)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&ctx->counters, 16 * sizeof(unsigned long long))) != cudaSuccess) return fail(e);
+    if ((e = cudaMallocHost(&ctx->h_counters, 16 * sizeof(unsigned long long))) != cudaSuccess) return fail(e);
+    *out = ctx;
+    return XM_OK;
+}
+
+static void free_result(xm_ctx *ctx)
+{
+    xm_dev_free(ctx, ctx->res.pairs);
+    xm_dev_free(ctx, ctx->res.dist);
+    xm_dev_free(ctx, ctx->res.job);
+    xm_dev_free(ctx, ctx->res.pairs_g);
+    xm_dev_free(ctx, ctx->res.dist_g);
+    ctx->res = xm_result_buf();
+}
+
+extern "C" xm_status xm_ctx_destroy(xm_ctx *ctx)
+{
+    if (!ctx) return XM_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_result(ctx);
+    for (auto &kv : ctx->alpha_cache) xm_dev_free(ctx, kv.second.dev);
+    xm_dev_free(ctx, ctx->d_jobs);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->counters) cudaFree(ctx->counters);
+    if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+    for (auto &ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return XM_OK;
+}
+
+extern "C" xm_status xm_ctx_info(const xm_ctx *ctx, int *device, int *sm_count, uint64_t *free_bytes,
+                                 uint64_t *total_bytes)
+{
+    if (!ctx) return XM_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    size_t f = 0, t = 0;
+    cudaMemGetInfo(&f, &t);
+    if (device) *device = ctx->device;
+    if (sm_count) *sm_count = ctx->sm_count;
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return XM_OK;
+}
+
+extern "C" xm_status xm_ctx_stream(const xm_ctx *ctx, void **stream)
+{
+    if (!ctx || !stream) return XM_ERR_INVALID;
+    *stream = (void *)ctx->stream;
+    return XM_OK;
+}
+
+extern "C" xm_status xm_ctx_synchronize(xm_ctx *ctx)
+{
+    if (!ctx) return XM_ERR_INVALID;
+    XM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return XM_OK;
+}
+
+xm_status xm_get_alpha(xm_ctx *ctx, double sr_deg, double zh_deg, int32_t n_zones, const double **dev_alpha)
+{
+    uint64_t a, b;
+    std::memcpy(&a, &sr_deg, 8);
+    std::memcpy(&b, &zh_deg, 8);
+    uint64_t key = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull + (a << 6) + (a >> 2));
+    auto it = ctx->alpha_cache.find(key);
+    if (it != ctx->alpha_cache.end() && it->second.n_zones == n_zones) {
+        *dev_alpha = it->second.dev;
+        return XM_OK;
+    }
+    if (ctx->alpha_cache.size() > 64) {
+        for (auto &kv : ctx->alpha_cache) xm_dev_free(ctx, kv.second.dev);
+        ctx->alpha_cache.clear();
+    }
+    std::vector<double> h((size_t)n_zones);
+    xm_host_alpha_table(sr_deg, zh_deg, n_zones, h.data());
+    xm_alpha_entry e;
+    e.n_zones = n_zones;
+    XM_TRY(xm_dev_alloc(ctx, (void **)&e.dev, (size_t)n_zones * 8));
+    XM_CUDA(ctx, cudaMemcpyAsync(e.dev, h.data(), (size_t)n_zones * 8, cudaMemcpyHostToDevice, ctx->stream));
+    XM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // h goes out of scope
+    ctx->alpha_cache[key] = e;
+    *dev_alpha = e.dev;
+    return XM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// segments
+// ---------------------------------------------------------------------------
+static xm_status new_segment(xm_ctx *ctx, uint32_t seg_id, double zh_deg, xm_segment **out)
+{
+    if (!(zh_deg > 0) || !std::isfinite(zh_deg)) return XM_ERR_INVALID;
+    double nzd = std::ceil(180 / zh_deg);
+    if (nzd > 2.0e9) {
+        ctx->last_error = "zone height too small";
+        return XM_ERR_INVALID;
+    }
+    xm_segment *s = new xm_segment();
+    s->ctx = ctx;
+    s->seg_id = seg_id;
+    s->zh_deg = zh_deg;
+    s->n_zones = zones_for(zh_deg);
+    *out = s;
+    return XM_OK;
+}
+
+extern "C" xm_status xm_segment_build_device(xm_ctx *ctx, uint32_t seg_id, const xm_obj *dev_objs, uint64_t n,
+                                             double zh_deg, xm_segment **out, xm_stats *stats)
+{
+    if (!ctx || !out || (n && !dev_objs)) return XM_ERR_INVALID;
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    xm_segment *s = nullptr;
+    XM_TRY(new_segment(ctx, seg_id, zh_deg, &s));
+    xm_status rc = xm_build_impl(s, dev_objs, n, stats);
+    if (rc != XM_OK) {
+        xm_segment_free(s);
+        return rc;
+    }
+    *out = s;
+    return XM_OK;
+}
+
+extern "C" xm_status xm_segment_rebuild_device(xm_segment *seg, const xm_obj *dev_objs, uint64_t n,
+                                               xm_stats *stats)
+{
+    if (!seg || (n && !dev_objs)) return XM_ERR_INVALID;
+    cudaSetDevice(seg->ctx->device);
+    return xm_build_impl(seg, dev_objs, n, stats);
+}
+
+extern "C" xm_status xm_segment_build(xm_ctx *ctx, uint32_t seg_id, const xm_obj *host_objs, uint64_t n,
+                                      double zh_deg, xm_segment **out, xm_stats *stats)
+{
+    if (!ctx || !out || (n && !host_objs)) return XM_ERR_INVALID;
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    xm_segment *s = nullptr;
+    XM_TRY(new_segment(ctx, seg_id, zh_deg, &s));
+    void *d = nullptr;
+    xm_status rc = xm_dev_alloc(ctx, &d, std::max<uint64_t>(n, 1) * sizeof(xm_obj));
+    if (rc == XM_OK && n) {
+        if (stats) cudaEventRecord(ctx->ev[12], ctx->stream);
+        cudaError_t e = cudaMemcpyAsync(d, host_objs, n * sizeof(xm_obj), cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) {
+            ctx->last_error = cudaGetErrorString(e);
+            rc = XM_ERR_CUDA;
+        }
+        if (stats) cudaEventRecord(ctx->ev[13], ctx->stream);
+    }
+    if (rc == XM_OK) rc = xm_build_impl(s, (const xm_obj *)d, n, stats);
+    if (rc == XM_OK && n && stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[12], ctx->ev[13]);   // build_impl synchronised the stream
+        stats->ms_h2d += ms;
+    }
+    xm_dev_free(ctx, d);
+    if (rc != XM_OK) {
+        xm_segment_free(s);
+        return rc;
+    }
+    *out = s;
+    return XM_OK;
+}
+
+extern "C" xm_status xm_segment_free(xm_segment *seg)
+{
+    if (!seg) return XM_OK;
+    xm_ctx *ctx = seg->ctx;
+    cudaSetDevice(ctx->device);
+    xm_dev_free(ctx, seg->zone_off);
+    xm_dev_free(ctx, seg->id);
+    xm_dev_free(ctx, seg->radec);
+    xm_dev_free(ctx, seg->xyz);
+    xm_dev_free(ctx, seg->tmp);
+    xm_dev_free(ctx, seg->cnt);
+    xm_dev_free(ctx, seg->scan_tmp);
+    xm_dev_free(ctx, seg->big);
+    delete seg;
+    return XM_OK;
+}
+
+extern "C" xm_status xm_segment_info(const xm_segment *seg, uint32_t *seg_id, uint64_t *n_kept, int32_t *n_zones,
+                                     double *zh_deg)
+{
+    if (!seg) return XM_ERR_INVALID;
+    if (seg_id) *seg_id = seg->seg_id;
+    if (n_kept) *n_kept = seg->n;
+    if (n_zones) *n_zones = seg->n_zones;
+    if (zh_deg) *zh_deg = seg->zh_deg;
+    return XM_OK;
+}
+
+extern "C" xm_status xm_segment_export(const xm_segment *seg, int64_t *id, double *radec, int32_t *zone_begin,
+                                       int32_t *zone_end)
+{
+    if (!seg) return XM_ERR_INVALID;
+    xm_ctx *ctx = seg->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    if (id && seg->n) XM_CUDA(ctx, cudaMemcpyAsync(id, seg->id, seg->n * 8, cudaMemcpyDeviceToHost, st));
+    if (radec && seg->n) XM_CUDA(ctx, cudaMemcpyAsync(radec, seg->radec, seg->n * 16, cudaMemcpyDeviceToHost, st));
+    if (zone_begin || zone_end) {
+        std::vector<uint32_t> z((size_t)seg->n_zones + 1);
+        XM_CUDA(ctx, cudaMemcpyAsync(z.data(), seg->zone_off, z.size() * 4, cudaMemcpyDeviceToHost, st));
+        XM_CUDA(ctx, cudaStreamSynchronize(st));
+        for (int32_t k = 0; k < seg->n_zones; ++k) {
+            if (zone_begin) zone_begin[k] = (int32_t)z[k];
+            if (zone_end) zone_end[k] = (int32_t)z[k + 1];
+        }
+    }
+    XM_CUDA(ctx, cudaStreamSynchronize(st));
+    return XM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// matching
+// ---------------------------------------------------------------------------
+namespace {
+
+xm_status ensure_result(xm_ctx *ctx, uint64_t cap, bool want_job)
+{
+    xm_result_buf &r = ctx->res;
+    if (r.cap >= cap && r.pairs && (!want_job || r.job)) return XM_OK;
+    uint64_t c = std::max<uint64_t>(cap, r.cap);
+    xm_dev_free(ctx, r.pairs);
+    xm_dev_free(ctx, r.dist);
+    xm_dev_free(ctx, r.job);
+    r.pairs = nullptr; r.dist = nullptr; r.job = nullptr; r.cap = 0;
+    XM_TRY(xm_dev_alloc(ctx, (void **)&r.pairs, c * 16));
+    XM_TRY(xm_dev_alloc(ctx, (void **)&r.dist, c * 8));
+    XM_TRY(xm_dev_alloc(ctx, (void **)&r.job, c * 4));
+    r.cap = c;
+    return XM_OK;
+}
+
+struct Prepared {
+    std::vector<xm::JobDev> jobs;
+    uint32_t n_tiles = 0;
+    uint64_t cap_guess = 0;
+};
+
+xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, int tile, Prepared &P)
+{
+    P.jobs.resize(n_jobs);
+    uint64_t tiles = 0, guess = 0;
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        const xm_segment *A = jobs[j].A, *B = jobs[j].B;
+        if (!A || !B || A->ctx != ctx || B->ctx != ctx) {
+            ctx->last_error = "job " + std::to_string(j) + ": missing segment or segment of another context";
+            return XM_ERR_INVALID;
+        }
+        if (A->zh_deg != B->zh_deg || A->n_zones != B->n_zones) {
+            ctx->last_error = "job " + std::to_string(j) + ": zone heights differ";
+            return XM_ERR_MISMATCH;
+        }
+        xm_match_params p;
+        if (xm_make_params(jobs[j].sr_deg, A->zh_deg, &p) != XM_OK) {
+            ctx->last_error = "job " + std::to_string(j) + ": invalid radius";
+            return XM_ERR_INVALID;
+        }
+        const double *alpha = nullptr;
+        XM_TRY(xm_get_alpha(ctx, p.sr_deg, A->zh_deg, A->n_zones, &alpha));
+        xm::JobDev &d = P.jobs[j];
+        std::memset(&d, 0, sizeof(d));
+        d.a_id = (const long long *)A->id;
+        d.a_radec = A->radec;
+        d.a_xyz = A->xyz;
+        d.b_id = (const long long *)B->id;
+        d.b_radec = B->radec;
+        d.b_xyz = B->xyz;
+        d.b_zoff = B->zone_off;
+        d.alpha = alpha;
+        d.sr_rad = p.sr_rad;
+        d.sr_dist2 = p.sr_dist2;
+        d.thr_hi = p.thr_hi;
+        d.thr_lo = p.thr_lo;
+        d.n_zones = A->n_zones;
+        d.nz = p.nz;
+        d.nA = (uint32_t)A->n;
+        d.tile_begin = (uint32_t)tiles;
+        tiles += (A->n + tile - 1) / tile;
+        guess += 2 * std::max(A->n, B->n);   // Worker.cu:296-297 default
+        if (tiles >= 0xFFFFFFF0ull) {
+            ctx->last_error = "too many tiles in one launch";
+            return XM_ERR_INVALID;
+        }
+    }
+    P.n_tiles = (uint32_t)tiles;
+    P.cap_guess = std::max<uint64_t>(guess, 1 << 16);
+    return XM_OK;
+}
+
+}  // namespace
+
+// Runs the pair kernel over the jobs; on return ctx->res holds the matches
+// (ungrouped) and ctx->h_counters the statistics.
+xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags, const xm_tuning *tuning,
+                      bool want_job, xm_stats *stats, float *kernel_ms)
+{
+    cudaStream_t st = ctx->stream;
+    xm::LaunchCfg L;
+    L.sm_count = ctx->sm_count;
+    L.variant = (flags & XM_PLAIN64) ? 1 : 0;
+    L.count_cand = (flags & XM_COUNT_CAND) != 0;
+    L.dist = (flags & XM_NO_DIST) == 0;
+    if (tuning) {
+        if (tuning->tile) L.tile = (int)tuning->tile;
+        if (tuning->chunk) L.chunk = tuning->chunk;
+        if (tuning->blocks_per_sm) L.blocks_per_sm = (int)tuning->blocks_per_sm;
+    }
+    if (L.tile != 64 && L.tile != 128 && L.tile != 256) return XM_ERR_INVALID;
+    Prepared P;
+    XM_TRY(prepare_jobs(ctx, jobs, n_jobs, L.tile, P));
+    size_t jb = P.jobs.size() * sizeof(xm::JobDev);
+    if (ctx->d_jobs_bytes < jb) {
+        xm_dev_free(ctx, ctx->d_jobs);
+        ctx->d_jobs = nullptr;
+        ctx->d_jobs_bytes = 0;
+        XM_TRY(xm_dev_alloc(ctx, &ctx->d_jobs, jb));
+        ctx->d_jobs_bytes = jb;
+    }
+    XM_CUDA(ctx, cudaMemcpyAsync(ctx->d_jobs, P.jobs.data(), jb, cudaMemcpyHostToDevice, st));
+    XM_TRY(ensure_result(ctx, std::max<uint64_t>(ctx->res.cap, P.cap_guess), want_job));
+    uint32_t retries = 0;
+    float ms = 0;
+    for (;;) {
+        XM_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16 * sizeof(unsigned long long), st));
+        xm::MatchOut out;
+        out.pairs = (long long *)ctx->res.pairs;
+        out.dist = L.dist ? ctx->res.dist : nullptr;
+        out.job = want_job ? ctx->res.job : nullptr;
+        out.cap = ctx->res.cap;
+        out.counters = ctx->counters;
+        XM_CUDA(ctx, cudaEventRecord(ctx->ev[2], st));
+        if (P.n_tiles > 0) XM_CUDA(ctx, xm::launch_pairs(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_tiles, out, st));
+        XM_CUDA(ctx, cudaEventRecord(ctx->ev[3], st));
+        XM_CUDA(ctx, cudaMemcpyAsync(ctx->h_counters, ctx->counters, 16 * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, st));
+        XM_CUDA(ctx, cudaStreamSynchronize(st));
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        uint64_t found = ctx->h_counters[0];
+        if (found <= ctx->res.cap) break;
+        // never truncate: grow to the exact count and run again
+        retries++;
+        uint64_t want = found + found / 16 + 1024;
+        xm_dev_free(ctx, ctx->res.pairs);
+        xm_dev_free(ctx, ctx->res.dist);
+        xm_dev_free(ctx, ctx->res.job);
+        ctx->res.pairs = nullptr; ctx->res.dist = nullptr; ctx->res.job = nullptr; ctx->res.cap = 0;
+        XM_TRY(ensure_result(ctx, want, want_job));
+    }
+    ctx->res.count = ctx->h_counters[0];
+    ctx->res.grouped = false;
+    ctx->res.has_dist = L.dist;
+    if (kernel_ms) *kernel_ms = ms;
+    if (stats) {
+        stats->n_match += ctx->h_counters[0];
+        stats->n_tested += ctx->h_counters[2];
+        stats->n_cand += ctx->h_counters[3];
+        stats->n_border += ctx->h_counters[4];
+        stats->n_exact += ctx->h_counters[5];
+        stats->n_tiles += P.n_tiles;
+        stats->n_launches += (P.n_tiles > 0 ? 1 : 0) * (retries + 1);
+        stats->n_retries += retries;
+        stats->ms_match += ms;
+    }
+    return XM_OK;
+}
+
+static xm_status copy_out(xm_ctx *ctx, const int64_t *dpairs, const double *ddist, uint64_t count, xm_pairs *out,
+                          xm_stats *stats)
+{
+    out->count = count;
+    if (!out->pairs && !out->dist) return XM_OK;
+    if (out->capacity < count) return XM_ERR_CAPACITY;
+    cudaStream_t st = ctx->stream;
+    XM_CUDA(ctx, cudaEventRecord(ctx->ev[4], st));
+    if (out->pairs && count) XM_CUDA(ctx, cudaMemcpyAsync(out->pairs, dpairs, count * 16, cudaMemcpyDeviceToHost, st));
+    if (out->dist && count) {
+        if (!ctx->res.has_dist) return XM_ERR_INVALID;
+        XM_CUDA(ctx, cudaMemcpyAsync(out->dist, ddist, count * 8, cudaMemcpyDeviceToHost, st));
+    }
+    XM_CUDA(ctx, cudaEventRecord(ctx->ev[5], st));
+    XM_CUDA(ctx, cudaStreamSynchronize(st));
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+        stats->ms_d2h += ms;
+    }
+    return XM_OK;
+}
+
+extern "C" xm_status xm_match(xm_ctx *ctx, const xm_segment *A, const xm_segment *B, double sr_deg, uint32_t flags,
+                              xm_pairs *out, xm_stats *stats)
+{
+    if (!ctx || !A || !B) return XM_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    xm_job job = {A, B, sr_deg};
+    XM_CUDA(ctx, cudaEventRecord(ctx->ev[6], ctx->stream));
+    XM_TRY(xm_run_jobs(ctx, &job, 1, flags, nullptr, false, stats, nullptr));
+    if (out) XM_TRY(copy_out(ctx, ctx->res.pairs, ctx->res.dist, ctx->res.count, out, stats));
+    if (stats) {
+        XM_CUDA(ctx, cudaEventRecord(ctx->ev[7], ctx->stream));
+        XM_CUDA(ctx, cudaEventSynchronize(ctx->ev[7]));
+        cudaEventElapsedTime(&stats->ms_total, ctx->ev[6], ctx->ev[7]);
+    }
+    return XM_OK;
+}
+
+extern "C" xm_status xm_fetch_pairs(xm_ctx *ctx, xm_pairs *out)
+{
+    if (!ctx || !out) return XM_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    const int64_t *p = ctx->res.grouped ? ctx->res.pairs_g : ctx->res.pairs;
+    const double *d = ctx->res.grouped ? ctx->res.dist_g : ctx->res.dist;
+    uint64_t n = std::min<uint64_t>(ctx->res.count, out->capacity);
+    uint64_t total = ctx->res.count;
+    xm_status rc = copy_out(ctx, p, d, n, out, nullptr);
+    out->count = total;
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// utilities
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void unit_vectors_kernel(const double *ra_deg, const double *dec_deg, uint64_t n, double *xyz)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        double x, y, z;
+        xm::radec2xyz(__ddiv_rn(ra_deg[i], XM_RAD2DEG), __ddiv_rn(dec_deg[i], XM_RAD2DEG), x, y, z);
+        xyz[3 * i] = x;
+        xyz[3 * i + 1] = y;
+        xyz[3 * i + 2] = z;
+    }
+}
+}  // namespace
+
+extern "C" xm_status xm_unit_vectors(xm_ctx *ctx, const double *ra_deg, const double *dec_deg, uint64_t n,
+                                     double *xyz)
+{
+    if (!ctx || (n && (!ra_deg || !dec_deg || !xyz))) return XM_ERR_INVALID;
+    if (!n) return XM_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    void *buf = nullptr;
+    XM_TRY(xm_dev_alloc(ctx, &buf, n * 40));
+    double *dra = (double *)buf, *dde = dra + n, *dx = dde + n;
+    xm_status rc = XM_OK;
+    if (cudaMemcpyAsync(dra, ra_deg, n * 8, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(dde, dec_deg, n * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        rc = XM_ERR_CUDA;
+    } else {
+        unit_vectors_kernel<<<(unsigned)std::min<uint64_t>((n + 255) / 256, 4096), 256, 0, st>>>(dra, dde, n, dx);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(xyz, dx, n * 24, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            rc = XM_ERR_CUDA;
+    }
+    cudaStreamSynchronize(st);
+    xm_dev_free(ctx, buf);
+    cudaStreamSynchronize(st);
+    return rc;
+}
+
+extern "C" xm_status xm_alpha_table(double sr_deg, double zh_deg, double *alpha, int32_t n_zones)
+{
+    if (!alpha || !(sr_deg > 0) || !(zh_deg > 0) || n_zones < 0) return XM_ERR_INVALID;
+    xm_host_alpha_table(sr_deg, zh_deg, n_zones, alpha);
+    return XM_OK;
+}

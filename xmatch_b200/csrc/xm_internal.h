@@ -1,0 +1,112 @@
+// xm_internal.h -- library-private types of libxmatch_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/xmatch.h"
+
+struct xm_alpha_entry {
+    double *dev = nullptr;   // [n_zones] RA half-width per zone (radians, 180 = no cut)
+    int32_t n_zones = 0;
+};
+
+// Device result of the last match call (library-owned, grown on demand).
+struct xm_result_buf {
+    int64_t *pairs = nullptr;   // [2 * cap] (idA, idB)
+    double *dist = nullptr;     // [cap]
+    uint32_t *job = nullptr;    // [cap] job index (batches)
+    uint64_t cap = 0;
+    uint64_t count = 0;         // matches of the last call
+    // batch grouping
+    int64_t *pairs_g = nullptr;
+    double *dist_g = nullptr;
+    uint64_t cap_g = 0;
+    std::vector<uint64_t> job_off;  // host copy, n_jobs + 1
+    bool grouped = false;
+    bool has_dist = true;
+};
+
+struct xm_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    cudaEvent_t ev[16] = {};
+    std::string last_error;
+    // counters: [0] matches, [1] tiles claimed, [2..] statistics
+    unsigned long long *counters = nullptr;   // device, 16 entries
+    unsigned long long *h_counters = nullptr; // pinned host mirror
+    std::unordered_map<uint64_t, xm_alpha_entry> alpha_cache;  // key: hash(sr, zh)
+    xm_result_buf res;
+    // job table for batches
+    void *d_jobs = nullptr;
+    size_t d_jobs_bytes = 0;
+    uint32_t *d_tile_begin = nullptr;
+    size_t d_tile_begin_n = 0;
+};
+
+struct xm_segment {
+    xm_ctx *ctx = nullptr;
+    uint32_t seg_id = 0;
+    uint64_t n_in = 0;        // records given
+    uint64_t n = 0;           // objects kept (valid zone)
+    uint64_t cap = 0;         // capacity of the SoA arrays
+    double zh_deg = 0;
+    int32_t n_zones = 0;
+    uint32_t *zone_off = nullptr;  // [n_zones + 2]; [n_zones + 1] = dropped count
+    int64_t *id = nullptr;
+    double2 *radec = nullptr;      // radians
+    float4 *xyz = nullptr;         // FP32 unit vector; w = zone id bits
+    // scratch kept for rebuilds
+    void *tmp = nullptr;           // 32-byte staging records
+    size_t tmp_bytes = 0;
+    uint32_t *cnt = nullptr;       // [n_zones + 2]
+    void *scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    uint32_t *big = nullptr;       // oversize chunk list
+    size_t big_cap = 0;
+};
+
+// ---- error plumbing ----
+#define XM_CUDA(ctx, call)                                                       \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            if (ctx) (ctx)->last_error = std::string(#call) + ": " + cudaGetErrorString(e_); \
+            return (e_ == cudaErrorMemoryAllocation) ? XM_ERR_NOMEM : XM_ERR_CUDA; \
+        }                                                                        \
+    } while (0)
+
+#define XM_TRY(call)                        \
+    do {                                    \
+        xm_status s_ = (call);              \
+        if (s_ != XM_OK) return s_;         \
+    } while (0)
+
+// ---- internal entry points shared between translation units ----
+xm_status xm_dev_alloc(xm_ctx *ctx, void **p, size_t bytes);
+void xm_dev_free(xm_ctx *ctx, void *p);
+xm_status xm_get_alpha(xm_ctx *ctx, double sr_deg, double zh_deg, int32_t n_zones,
+                       const double **dev_alpha);
+void xm_host_alpha_table(double sr_deg, double zh_deg, int32_t n_zones, double *out);
+
+// exclusive scan of n uint32 values (out[n] = total); tmp from xm_scan_tmp_bytes
+size_t xm_scan_tmp_bytes(size_t n);
+cudaError_t xm_scan_exclusive_u32(const uint32_t *in, uint32_t *out, size_t n, void *tmp,
+                                  cudaStream_t s);
+
+xm_status xm_build_impl(xm_segment *seg, const xm_obj *dev_objs, uint64_t n, xm_stats *st);
+
+// Match parameters derived on the host (Worker.cu:310-317).
+struct xm_match_params {
+    double sr_deg, sr_rad, sr_dist2;
+    float thr_hi;       // FP32 reject threshold: c32 > thr_hi => chord^2 >= sr_dist2
+    float thr_lo;       // c32 < thr_lo => chord^2 < sr_dist2 (statistics only)
+    int32_t nz;
+};
+xm_status xm_make_params(double sr_deg, double zh_deg, xm_match_params *p);

@@ -1,0 +1,48 @@
+// xm_match.cuh -- job table and launch description of the pair kernel.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace xm {
+
+// One segment-pair job (Job.h:16-29) as the pair kernel sees it.
+struct JobDev {
+    const long long *a_id;
+    const double2 *a_radec;
+    const float4 *a_xyz;
+    const long long *b_id;
+    const double2 *b_radec;
+    const float4 *b_xyz;
+    const uint32_t *b_zoff;    // [n_zones + 1]
+    const double *alpha;       // [n_zones] RA half-width of A's zones
+    double sr_rad, sr_dist2;
+    float thr_hi, thr_lo;
+    int n_zones, nz;
+    uint32_t nA;               // objects of A
+    uint32_t tile_begin;       // first global tile of this job
+    uint32_t pad[2];
+};
+
+struct MatchOut {
+    long long *pairs;          // [2 * cap]
+    double *dist;              // [cap] or null
+    uint32_t *job;             // [cap] or null
+    unsigned long long cap;
+    // [0] matches, [1] next tile, [2] tested, [3] candidates, [4] in margin band, [5] FP64 decisions
+    unsigned long long *counters;
+};
+
+struct LaunchCfg {
+    int tile = 128;            // A objects per tile = threads per block
+    uint32_t chunk = 4;        // tiles per work-stealing claim
+    int blocks_per_sm = 0;     // 0 = occupancy limit
+    int sm_count = 148;
+    int variant = 0;           // 0 FP32 reject + FP64 decision, 1 plain FP64
+    bool count_cand = false;
+    bool dist = true;
+};
+
+cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_tiles,
+                         const MatchOut &out, cudaStream_t st);
+
+}  // namespace xm
