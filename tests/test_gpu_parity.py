@@ -161,13 +161,15 @@ def test_tuning_does_not_change_results(ctx, fixtures, tile, chunk):
     check_parity(ctx, a, a, 5, variants=(0,), tuning=(tile, chunk, 0))
 
 
-def test_output_growth_never_truncates(ctx):
+def test_output_growth_never_truncates():
     # 2,500 sources inside 20": every pair matches at r = 60" (6.25 M pairs,
-    # far beyond the initial 2 * max(nA, nB) buffer)
+    # far beyond the initial 2 * max(nA, nB) buffer of a fresh context)
+    import xmatch_b200 as xm
     rng = np.random.default_rng(15)
     n = 2500
     A = objs(np.arange(n), 100 + rng.uniform(0, 20 * ARCSEC, n), 20 + rng.uniform(0, 20 * ARCSEC, n))
-    p, d, st = run_gpu(ctx, A, A, 60)
+    with xm.Context(0) as fresh:
+        p, d, st = run_gpu(fresh, A, A, 60)
     assert len(p) == n * n
     assert st["n_retries"] >= 1
     po, do, _ = oracle.xmatch(A, A, 60 * ARCSEC)
