@@ -155,10 +155,10 @@ def test_duplicate_coordinates(ctx):
     check_parity(ctx, A, A, 1, variants=(0,))
 
 
-@pytest.mark.parametrize("tile,chunk", [(64, 1), (128, 4), (256, 16)])
-def test_tuning_does_not_change_results(ctx, fixtures, tile, chunk):
+@pytest.mark.parametrize("tile,chunk,zones", [(64, 1, 1), (128, 4, 16), (256, 2, 64)])
+def test_tuning_does_not_change_results(ctx, fixtures, tile, chunk, zones):
     a, _ = fixtures
-    check_parity(ctx, a, a, 5, variants=(0,), tuning=(tile, chunk, 0))
+    check_parity(ctx, a, a, 5, variants=(0,), tuning=(tile, chunk, 0, zones))
 
 
 def test_output_growth_never_truncates():

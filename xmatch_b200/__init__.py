@@ -263,7 +263,7 @@ class Context:
         bms, fms = ctypes.c_float(), ctypes.c_float()
         _check(_lib.xm_autotune_batch(self._h, arr, len(jobs), flags, ctypes.byref(best), ctypes.byref(bms),
                                       ctypes.byref(fms)), self._h)
-        return (best.tile, best.chunk, best.blocks_per_sm), bms.value, fms.value
+        return (best.tile, best.chunk, best.blocks_per_sm, best.zones), bms.value, fms.value
 
     def unit_vectors(self, ra_deg, dec_deg):
         ra = np.ascontiguousarray(ra_deg, np.float64)

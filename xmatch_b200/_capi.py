@@ -52,7 +52,8 @@ class XmStats(ctypes.Structure):
 
 
 class XmTuning(ctypes.Structure):
-    _fields_ = [("tile", ctypes.c_uint32), ("chunk", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32)]
+    _fields_ = [("tile", ctypes.c_uint32), ("chunk", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
+                ("zones", ctypes.c_uint32)]
 
 
 class XmJob(ctypes.Structure):

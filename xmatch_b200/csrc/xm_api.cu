@@ -418,14 +418,14 @@ xm_status ensure_result(xm_ctx *ctx, uint64_t cap, bool want_job)
 
 struct Prepared {
     std::vector<xm::JobDev> jobs;
-    uint32_t n_tiles = 0;
+    uint32_t n_items = 0;
     uint64_t cap_guess = 0;
 };
 
-xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, int tile, Prepared &P)
+xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t zc, Prepared &P)
 {
     P.jobs.resize(n_jobs);
-    uint64_t tiles = 0, guess = 0;
+    uint64_t items = 0, guess = 0;
     for (uint32_t j = 0; j < n_jobs; ++j) {
         const xm_segment *A = jobs[j].A, *B = jobs[j].B;
         if (!A || !B || A->ctx != ctx || B->ctx != ctx) {
@@ -448,6 +448,7 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, int til
         d.a_id = (const long long *)A->id;
         d.a_radec = A->radec;
         d.a_xyz = A->xyz;
+        d.a_zoff = A->zone_off;
         d.b_id = (const long long *)B->id;
         d.b_radec = B->radec;
         d.b_xyz = B->xyz;
@@ -459,16 +460,18 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, int til
         d.thr_lo = p.thr_lo;
         d.n_zones = A->n_zones;
         d.nz = p.nz;
+        d.z_lo = A->z_lo;
+        d.z_hi = A->z_hi;
         d.nA = (uint32_t)A->n;
-        d.tile_begin = (uint32_t)tiles;
-        tiles += (A->n + tile - 1) / tile;
+        d.item_begin = (uint32_t)items;
+        if (A->n > 0 && B->n > 0 && A->z_hi >= A->z_lo) items += ((uint64_t)(A->z_hi - A->z_lo) + zc) / zc;
         guess += 2 * std::max(A->n, B->n);   // Worker.cu:296-297 default
-        if (tiles >= 0xFFFFFFF0ull) {
-            ctx->last_error = "too many tiles in one launch";
+        if (items >= 0xFFFFFF00ull) {
+            ctx->last_error = "too many work items in one launch";
             return XM_ERR_INVALID;
         }
     }
-    P.n_tiles = (uint32_t)tiles;
+    P.n_items = (uint32_t)items;
     P.cap_guess = std::max<uint64_t>(guess, 1 << 16);
     return XM_OK;
 }
@@ -490,10 +493,12 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         if (tuning->tile) L.tile = (int)tuning->tile;
         if (tuning->chunk) L.chunk = tuning->chunk;
         if (tuning->blocks_per_sm) L.blocks_per_sm = (int)tuning->blocks_per_sm;
+        if (tuning->zones) L.zc = tuning->zones;
     }
     if (L.tile != 64 && L.tile != 128 && L.tile != 256) return XM_ERR_INVALID;
+    if (L.zc < 1 || L.zc > 64 || L.chunk < 1) return XM_ERR_INVALID;
     Prepared P;
-    XM_TRY(prepare_jobs(ctx, jobs, n_jobs, L.tile, P));
+    XM_TRY(prepare_jobs(ctx, jobs, n_jobs, L.zc, P));
     size_t jb = P.jobs.size() * sizeof(xm::JobDev);
     if (ctx->d_jobs_bytes < jb) {
         xm_dev_free(ctx, ctx->d_jobs);
@@ -515,12 +520,17 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         out.cap = ctx->res.cap;
         out.counters = ctx->counters;
         XM_CUDA(ctx, cudaEventRecord(ctx->ev[2], st));
-        if (P.n_tiles > 0) XM_CUDA(ctx, xm::launch_pairs(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_tiles, out, st));
+        if (P.n_items > 0)
+            XM_CUDA(ctx, xm::launch_pairs(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_items, out, st));
         XM_CUDA(ctx, cudaEventRecord(ctx->ev[3], st));
         XM_CUDA(ctx, cudaMemcpyAsync(ctx->h_counters, ctx->counters, 16 * sizeof(unsigned long long),
                                      cudaMemcpyDeviceToHost, st));
         XM_CUDA(ctx, cudaStreamSynchronize(st));
         cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        if (ctx->h_counters[7]) {
+            ctx->last_error = "pair kernel: a bounded wait for staged data ran out";
+            return XM_ERR_TIMEOUT;
+        }
         uint64_t found = ctx->h_counters[0];
         if (found <= ctx->res.cap) break;
         // never truncate: grow to the exact count and run again
@@ -542,8 +552,8 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         stats->n_cand += ctx->h_counters[3];
         stats->n_border += ctx->h_counters[4];
         stats->n_exact += ctx->h_counters[5];
-        stats->n_tiles += P.n_tiles;
-        stats->n_launches += (P.n_tiles > 0 ? 1 : 0) * (retries + 1);
+        stats->n_tiles += P.n_items;
+        stats->n_launches += (P.n_items > 0 ? 1 : 0) * (retries + 1);
         stats->n_retries += retries;
         stats->ms_match += ms;
     }

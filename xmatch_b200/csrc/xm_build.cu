@@ -63,6 +63,15 @@ __global__ void zb_count(const xm_obj *__restrict__ objs, unsigned long long n, 
         }
         unsigned peers = __match_any_sync(0xffffffffu, bin);
         if (bin >= 0 && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&cnt[bin], (uint32_t)__popc(peers));
+        // populated zone range
+        unsigned zlo = (bin >= 0 && bin < n_zones) ? (unsigned)bin : 0xFFFFFFFFu;
+        unsigned zhi = (bin >= 0 && bin < n_zones) ? (unsigned)bin : 0u;
+        zlo = __reduce_min_sync(0xffffffffu, zlo);
+        zhi = __reduce_max_sync(0xffffffffu, zhi);
+        if (lane == 0) {
+            if (zlo != 0xFFFFFFFFu) atomicMin(&cnt[n_zones + 2], zlo);
+            atomicMax(&cnt[n_zones + 3], zhi);
+        }
     }
 }
 
@@ -443,7 +452,7 @@ xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stat
         seg->cap = c;
     }
     if (!seg->zone_off) XM_TRY(xm_dev_alloc(ctx, (void **)&seg->zone_off, ((size_t)nz + 2) * 4));
-    if (!seg->cnt) XM_TRY(xm_dev_alloc(ctx, (void **)&seg->cnt, ((size_t)nz + 2) * 4));
+    if (!seg->cnt) XM_TRY(xm_dev_alloc(ctx, (void **)&seg->cnt, ((size_t)nz + 4) * 4));
     XM_TRY(ensure(ctx, &seg->tmp, &seg->tmp_bytes, std::max<uint64_t>(n, 1) * sizeof(StageRec)));
     XM_TRY(ensure(ctx, &seg->scan_tmp, &seg->scan_tmp_bytes, xm_scan_tmp_bytes((size_t)nz)));
     const uint32_t big_cap = 4096;
@@ -454,7 +463,8 @@ xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stat
     StageRec *stage = (StageRec *)seg->tmp;
 
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[0], st));
-    XM_CUDA(ctx, cudaMemsetAsync(seg->cnt, 0, ((size_t)nz + 2) * 4, st));
+    XM_CUDA(ctx, cudaMemsetAsync(seg->cnt, 0, ((size_t)nz + 4) * 4, st));
+    XM_CUDA(ctx, cudaMemsetAsync(seg->cnt + nz + 2, 0xFF, 4, st));
     XM_CUDA(ctx, cudaMemsetAsync(seg->big, 0, 4, st));
     const int threads = 256;
     int g = grid_for(n, threads, ctx->sm_count);
@@ -488,12 +498,20 @@ xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stat
         if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[11], st));
     }
     // kept / dropped counts and the oversize list
-    uint32_t h[3];
+    uint32_t h[5];
     XM_CUDA(ctx, cudaMemcpyAsync(&h[0], seg->zone_off + nz, 8, cudaMemcpyDeviceToHost, st));
     XM_CUDA(ctx, cudaMemcpyAsync(&h[2], seg->big, 4, cudaMemcpyDeviceToHost, st));
+    XM_CUDA(ctx, cudaMemcpyAsync(&h[3], seg->cnt + nz + 2, 8, cudaMemcpyDeviceToHost, st));
     XM_CUDA(ctx, cudaStreamSynchronize(st));
     seg->n = h[0];
     seg->n_in = n;
+    if (seg->n > 0) {
+        seg->z_lo = (int32_t)h[3];
+        seg->z_hi = (int32_t)h[4];
+    } else {
+        seg->z_lo = 0;
+        seg->z_hi = -1;
+    }
     if (h[2] > 0) {
         uint32_t nbig = h[2];
         std::vector<uint32_t> chunks;

@@ -58,6 +58,7 @@ struct xm_segment {
     uint64_t cap = 0;         // capacity of the SoA arrays
     double zh_deg = 0;
     int32_t n_zones = 0;
+    int32_t z_lo = 0, z_hi = -1;   // first / last zone holding an object
     uint32_t *zone_off = nullptr;  // [n_zones + 2]; [n_zones + 1] = dropped count
     int64_t *id = nullptr;
     double2 *radec = nullptr;      // radians
@@ -65,7 +66,7 @@ struct xm_segment {
     // scratch kept for rebuilds
     void *tmp = nullptr;           // 32-byte staging records
     size_t tmp_bytes = 0;
-    uint32_t *cnt = nullptr;       // [n_zones + 2]
+    uint32_t *cnt = nullptr;       // [n_zones + 4]: histogram, dropped, -, min zone, max zone
     void *scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
     uint32_t *big = nullptr;       // oversize chunk list

@@ -10,6 +10,7 @@ struct JobDev {
     const long long *a_id;
     const double2 *a_radec;
     const float4 *a_xyz;
+    const uint32_t *a_zoff;    // [n_zones + 1]
     const long long *b_id;
     const double2 *b_radec;
     const float4 *b_xyz;
@@ -18,9 +19,9 @@ struct JobDev {
     double sr_rad, sr_dist2;
     float thr_hi, thr_lo;
     int n_zones, nz;
+    int z_lo, z_hi;            // populated zone range of A
     uint32_t nA;               // objects of A
-    uint32_t tile_begin;       // first global tile of this job
-    uint32_t pad[2];
+    uint32_t item_begin;       // first global work item of this job
 };
 
 struct MatchOut {
@@ -28,13 +29,15 @@ struct MatchOut {
     double *dist;              // [cap] or null
     uint32_t *job;             // [cap] or null
     unsigned long long cap;
-    // [0] matches, [1] next tile, [2] tested, [3] candidates, [4] in margin band, [5] FP64 decisions
+    // [0] matches, [1] next work item, [2] tested, [3] candidates, [4] in margin band,
+    // [5] FP64 decisions, [7] error flag (a bounded wait ran out)
     unsigned long long *counters;
 };
 
 struct LaunchCfg {
     int tile = 128;            // A objects per tile = threads per block
-    uint32_t chunk = 4;        // tiles per work-stealing claim
+    uint32_t zc = 16;          // zones per work item
+    uint32_t chunk = 2;        // work items per work-stealing claim
     int blocks_per_sm = 0;     // 0 = occupancy limit
     int sm_count = 148;
     int variant = 0;           // 0 FP32 reject + FP64 decision, 1 plain FP64
@@ -42,7 +45,7 @@ struct LaunchCfg {
     bool dist = true;
 };
 
-cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_tiles,
+cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items,
                          const MatchOut &out, cudaStream_t st);
 
 }  // namespace xm
