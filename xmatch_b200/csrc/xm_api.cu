@@ -200,6 +200,7 @@ extern "C" xm_status xm_ctx_destroy(xm_ctx *ctx)
     free_result(ctx);
     for (auto &kv : ctx->alpha_cache) xm_dev_free(ctx, kv.second.dev);
     xm_dev_free(ctx, ctx->d_jobs);
+    xm_dev_free(ctx, ctx->d_work);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->counters) cudaFree(ctx->counters);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
@@ -419,6 +420,7 @@ xm_status ensure_result(xm_ctx *ctx, uint64_t cap, bool want_job)
 struct Prepared {
     std::vector<xm::JobDev> jobs;
     uint32_t n_items = 0;
+    uint64_t total_a = 0;
     uint64_t cap_guess = 0;
 };
 
@@ -464,7 +466,10 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
         d.z_hi = A->z_hi;
         d.nA = (uint32_t)A->n;
         d.item_begin = (uint32_t)items;
-        if (A->n > 0 && B->n > 0 && A->z_hi >= A->z_lo) items += ((uint64_t)(A->z_hi - A->z_lo) + zc) / zc;
+        if (A->n > 0 && B->n > 0 && A->z_hi >= A->z_lo) {
+            items += ((uint64_t)(A->z_hi - A->z_lo) + zc) / zc;
+            P.total_a += A->n;
+        }
         guess += 2 * std::max(A->n, B->n);   // Worker.cu:296-297 default
         if (items >= 0xFFFFFF00ull) {
             ctx->last_error = "too many work items in one launch";
@@ -509,6 +514,28 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
     }
     XM_CUDA(ctx, cudaMemcpyAsync(ctx->d_jobs, P.jobs.data(), jb, cudaMemcpyHostToDevice, st));
     XM_TRY(ensure_result(ctx, std::max<uint64_t>(ctx->res.cap, P.cap_guess), want_job));
+    // tile pre-pass buffers
+    const uint64_t max_tiles = xm::plan_bound(P.n_items, P.total_a, L.tile);
+    if (max_tiles >= 0xFFFFFF00ull) {
+        ctx->last_error = "too many tiles in one launch";
+        return XM_ERR_INVALID;
+    }
+    const size_t cnt_b = ((size_t)P.n_items * 4 + 255) & ~(size_t)255;
+    const size_t off_b = ((size_t)(P.n_items + 1) * 4 + 255) & ~(size_t)255;
+    const size_t scan_b = (xm_scan_tmp_bytes(P.n_items) + 255) & ~(size_t)255;
+    const size_t need = cnt_b + off_b + scan_b + xm::plan_bytes(max_tiles) + 256;
+    if (ctx->d_work_bytes < need) {
+        xm_dev_free(ctx, ctx->d_work);
+        ctx->d_work = nullptr;
+        ctx->d_work_bytes = 0;
+        XM_TRY(xm_dev_alloc(ctx, &ctx->d_work, need + need / 4));
+        ctx->d_work_bytes = need + need / 4;
+    }
+    char *wp = (char *)ctx->d_work;
+    uint32_t *tile_cnt = (uint32_t *)wp;
+    uint32_t *tile_off = (uint32_t *)(wp + cnt_b);
+    void *scan_tmp = wp + cnt_b + off_b;
+    void *plans = wp + cnt_b + off_b + scan_b;
     uint32_t retries = 0;
     float ms = 0;
     for (;;) {
@@ -521,14 +548,15 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         out.counters = ctx->counters;
         XM_CUDA(ctx, cudaEventRecord(ctx->ev[2], st));
         if (P.n_items > 0)
-            XM_CUDA(ctx, xm::launch_pairs(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_items, out, st));
+            XM_CUDA(ctx, xm::launch_pairs(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_items, plans, tile_cnt,
+                                          tile_off, scan_tmp, (uint32_t)max_tiles, out, st));
         XM_CUDA(ctx, cudaEventRecord(ctx->ev[3], st));
         XM_CUDA(ctx, cudaMemcpyAsync(ctx->h_counters, ctx->counters, 16 * sizeof(unsigned long long),
                                      cudaMemcpyDeviceToHost, st));
         XM_CUDA(ctx, cudaStreamSynchronize(st));
         cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
         if (ctx->h_counters[7]) {
-            ctx->last_error = "pair kernel: a bounded wait for staged data ran out";
+            ctx->last_error = "pair kernel: a bounded wait for staged data ran out, or the tile plan overflowed";
             return XM_ERR_TIMEOUT;
         }
         uint64_t found = ctx->h_counters[0];
@@ -553,7 +581,7 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         stats->n_border += ctx->h_counters[4];
         stats->n_exact += ctx->h_counters[5];
         stats->n_tiles += P.n_items;
-        stats->n_launches += (P.n_items > 0 ? 1 : 0) * (retries + 1);
+        stats->n_launches += (P.n_items > 0 ? 6 : 0) * (retries + 1);   // count, 3 scan, plans, pairs
         stats->n_retries += retries;
         stats->ms_match += ms;
     }

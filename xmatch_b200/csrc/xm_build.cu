@@ -50,7 +50,14 @@ __device__ __forceinline__ unsigned lanemask_lt()
 __global__ void zb_count(const xm_obj *__restrict__ objs, unsigned long long n, double zh_deg,
                          int n_zones, uint32_t *__restrict__ cnt)
 {
+    __shared__ unsigned s_lo, s_hi;
+    if (threadIdx.x == 0) {
+        s_lo = 0xFFFFFFFFu;
+        s_hi = 0u;
+    }
+    __syncthreads();
     const unsigned lane = threadIdx.x & 31;
+    unsigned zlo = 0xFFFFFFFFu, zhi = 0u;   // populated zone range seen by this thread
     unsigned long long warp0 = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull;
     unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     for (unsigned long long base = warp0; base < n; base += stride) {
@@ -60,18 +67,24 @@ __global__ void zb_count(const xm_obj *__restrict__ objs, unsigned long long n, 
             const xm_obj o = objs[i];
             int z = isfinite(o.ra_deg) ? xm::zone_of(o.dec_deg, zh_deg, n_zones) : -1;
             bin = z < 0 ? n_zones : z;
+            if (z >= 0) {
+                zlo = min(zlo, (unsigned)z);
+                zhi = max(zhi, (unsigned)z);
+            }
         }
         unsigned peers = __match_any_sync(0xffffffffu, bin);
         if (bin >= 0 && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&cnt[bin], (uint32_t)__popc(peers));
-        // populated zone range
-        unsigned zlo = (bin >= 0 && bin < n_zones) ? (unsigned)bin : 0xFFFFFFFFu;
-        unsigned zhi = (bin >= 0 && bin < n_zones) ? (unsigned)bin : 0u;
-        zlo = __reduce_min_sync(0xffffffffu, zlo);
-        zhi = __reduce_max_sync(0xffffffffu, zhi);
-        if (lane == 0) {
-            if (zlo != 0xFFFFFFFFu) atomicMin(&cnt[n_zones + 2], zlo);
-            atomicMax(&cnt[n_zones + 3], zhi);
-        }
+    }
+    zlo = __reduce_min_sync(0xffffffffu, zlo);
+    zhi = __reduce_max_sync(0xffffffffu, zhi);
+    if (lane == 0) {
+        atomicMin(&s_lo, zlo);
+        atomicMax(&s_hi, zhi);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_lo != 0xFFFFFFFFu) atomicMin(&cnt[n_zones + 2], s_lo);
+        atomicMax(&cnt[n_zones + 3], s_hi);
     }
 }
 
@@ -446,12 +459,15 @@ xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stat
         seg->id = nullptr; seg->radec = nullptr; seg->xyz = nullptr;
         seg->cap = 0;
         uint64_t c = std::max<uint64_t>(n, 1);
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->id, c * sizeof(int64_t)));
+        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->id, (c + 2) * sizeof(int64_t)));
         XM_TRY(xm_dev_alloc(ctx, (void **)&seg->radec, c * sizeof(double2)));
         XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz, c * sizeof(float4)));
         seg->cap = c;
     }
-    if (!seg->zone_off) XM_TRY(xm_dev_alloc(ctx, (void **)&seg->zone_off, ((size_t)nz + 2) * 4));
+    if (!seg->zone_off) {
+        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->zone_off, ((size_t)nz + 8) * 4));
+        XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0, ((size_t)nz + 8) * 4, st));
+    }
     if (!seg->cnt) XM_TRY(xm_dev_alloc(ctx, (void **)&seg->cnt, ((size_t)nz + 4) * 4));
     XM_TRY(ensure(ctx, &seg->tmp, &seg->tmp_bytes, std::max<uint64_t>(n, 1) * sizeof(StageRec)));
     XM_TRY(ensure(ctx, &seg->scan_tmp, &seg->scan_tmp_bytes, xm_scan_tmp_bytes((size_t)nz)));

@@ -43,11 +43,11 @@ struct xm_ctx {
     unsigned long long *h_counters = nullptr; // pinned host mirror
     std::unordered_map<uint64_t, xm_alpha_entry> alpha_cache;  // key: hash(sr, zh)
     xm_result_buf res;
-    // job table for batches
+    // job table and tile pre-pass buffers
     void *d_jobs = nullptr;
     size_t d_jobs_bytes = 0;
-    uint32_t *d_tile_begin = nullptr;
-    size_t d_tile_begin_n = 0;
+    void *d_work = nullptr;      // tile counts, offsets, scan scratch, plans
+    size_t d_work_bytes = 0;
 };
 
 struct xm_segment {
@@ -55,11 +55,12 @@ struct xm_segment {
     uint32_t seg_id = 0;
     uint64_t n_in = 0;        // records given
     uint64_t n = 0;           // objects kept (valid zone)
-    uint64_t cap = 0;         // capacity of the SoA arrays
+    uint64_t cap = 0;         // capacity of the SoA arrays (id has 2 spare entries)
     double zh_deg = 0;
     int32_t n_zones = 0;
     int32_t z_lo = 0, z_hi = -1;   // first / last zone holding an object
-    uint32_t *zone_off = nullptr;  // [n_zones + 2]; [n_zones + 1] = dropped count
+    uint32_t *zone_off = nullptr;  // [n_zones + 8]; [n_zones + 1] = dropped count; the rest
+                                   // pads 16-byte bulk copies of zone-offset slices
     int64_t *id = nullptr;
     double2 *radec = nullptr;      // radians
     float4 *xyz = nullptr;         // FP32 unit vector; w = zone id bits

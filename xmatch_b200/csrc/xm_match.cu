@@ -5,21 +5,24 @@
 // all-pairs kernel xmatch_kernel (Worker.cu:65-241).
 //
 // Work decomposition.  A work item is `zc` consecutive zones of one job's A
-// segment; blocks claim `chunk` items at a time from a global counter.  A
-// block cuts its zones into tiles of at most TILE objects (one per thread):
-// a zone holding more than TILE/2 objects is split into near-equal
-// single-zone tiles, consecutive smaller zones are packed into one tile.
+// segment.  A pre-pass (one thread per item) cuts items into tiles of at
+// most TILE objects -- a zone holding more than TILE/2 objects is split into
+// near-equal single-zone tiles, consecutive smaller zones are packed into
+// one tile -- and writes a staging plan per tile:
+//   WHOLE   the B zones within nz of the tile's zones (Worker.cu:338-341) are
+//           one contiguous range of the zone-sorted B segment; copied whole;
+//   UNION   (a single-zone tile whose band is too large) per B zone only the
+//           union of the tile's RA windows, [ra_first - alpha, ra_last +
+//           alpha], when no RA-wraparound window can be non-empty;
+//   GLOBAL  neither fits: the windows are bisected in global memory.
 //
-// Staging.  For a tile, the B zones within nz of its zones (Worker.cu:
-// 338-341) are copied into shared memory with bulk asynchronous copies
-// (cp.async.bulk, completion on an mbarrier):
-//   * single-zone tile: per B zone only the union of the tile's RA windows,
-//     i.e. objects with ra in [ra_first - alpha, ra_last + alpha] (A is
-//     ra-sorted), unless an RA-wraparound window could be non-empty or alpha
-//     is the "no cut" sentinel, in which case the whole zone;
-//   * packed tile: the whole B zones.
-// Tiles whose staged set exceeds the buffer fall back to bisecting B in
-// global memory.
+// Pair kernel.  Warp-specialised and persistent: warp 0 claims tiles from a
+// global counter (`chunk` at a time) and streams each tile's A objects and
+// staged B ranges into a ring of shared-memory stages with bulk asynchronous
+// copies (cp.async.bulk, completion counted on an mbarrier; no multicast);
+// warps 1..TILE/32 consume a stage, one A object per thread, and release it
+// on an "empty" mbarrier.  Every wait is bounded; a timeout sets an error
+// flag that the host reports.
 //
 // Pair test.  Every thread bisects its own windows (direct, and the two
 // wrapped ones for the RA branches of Worker.cu:89,98,110) in the staged ra
@@ -31,9 +34,9 @@
 // bound proven to imply chord^2_FP64 >= threshold; every other pair is
 // decided by the FP64 predicate, so the pair set is the FP64 one bit for bit.
 //
-// Output.  Matches are compacted per warp with __ballot_sync/__popc into a
-// block buffer in shared memory that is appended to global memory with one
-// atomicAdd per flush (Worker.cu:128-240 uses two Hillis-Steele scans per
+// Output.  Matches are compacted per warp with __ballot_sync/__popc into the
+// warp's buffer in shared memory, which is appended to global memory with
+// one atomicAdd per flush (Worker.cu:128-240 uses two Hillis-Steele scans per
 // block).  A full output buffer is detected and reported, never silently
 // truncated (Worker.cu:147-148).
 #include <algorithm>
@@ -48,9 +51,6 @@ namespace xm {
 
 namespace {
 
-constexpr int kSbuf = 256;         // block output staging records
-constexpr int kStageCap = 1024;    // B objects staged per tile
-constexpr int kMaxSeg = 96;        // B zones per tile band
 constexpr double kWinEps = 1e-12;  // window widening (radians), >> FP64 rounding of ra +- alpha
 constexpr unsigned kWaitLimit = 1u << 26;   // bounded mbarrier wait (iterations)
 
@@ -149,17 +149,19 @@ struct AObj {
     bool have_xyz;
 };
 
-// View of B for window enumeration: either the staged copy in shared
-// memory (segments per band zone) or the segment in global memory.
+// View of B for window enumeration.
+//   WHOLE  (staged, whole): band zone zb -> [zoff[k] - base, zoff[k+1] - base),
+//          k = zb - band_lo, global index = base + q;
+//   UNION  (staged): band zone k -> [off[k], off[k+1]), global g[k] + (q - off[k]);
+//   global: zone zb -> [zoff[zb], zoff[zb+1]) of the segment itself.
 struct BView {
-    const double2 *radec;   // staged or global
+    const double2 *radec;
     const float4 *xyz;
-    bool staged;
-    // staged: band zone k -> [off[k], off[k+1]) in shared memory, global index g[k] + (q - off[k])
+    bool staged, whole;
+    int band_lo;
+    uint32_t base;
     const uint32_t *off;
     const uint32_t *g;
-    int band_lo;
-    // global
     const uint32_t *zoff;
 };
 
@@ -239,7 +241,11 @@ __device__ __forceinline__ bool next_candidate(const BView &V, const AObj &a, Cu
         }
         c.zb++;
         if (c.zb > c.zb_end) return false;
-        if (V.staged) {
+        if (V.whole) {
+            const int k = c.zb - V.band_lo;
+            c.b0 = V.zoff[k] - V.base;
+            c.b1 = V.zoff[k + 1] - V.base;
+        } else if (V.staged) {
             const int k = c.zb - V.band_lo;
             c.b0 = V.off[k];
             c.b1 = V.off[k + 1];
@@ -259,6 +265,7 @@ __device__ __forceinline__ bool next_candidate(const BView &V, const AObj &a, Cu
 
 __device__ __forceinline__ uint32_t global_index(const BView &V, int zb, uint32_t q)
 {
+    if (V.whole) return V.base + q;
     if (!V.staged) return q;
     const int k = zb - V.band_lo;
     return V.g[k] + (q - V.off[k]);
@@ -275,17 +282,29 @@ __device__ __forceinline__ bool cuts_pass(const JobDev &J, const AObj &a, double
     return fabs(d) < a.alpha || fabs(__dsub_rn(d, XM_TWO_PI)) < a.alpha || fabs(__dadd_rn(d, XM_TWO_PI)) < a.alpha;
 }
 
-struct SBuf {
-    longlong2 ab[kSbuf];
-    double d[kSbuf];
-    uint32_t job[kSbuf];
+__device__ __forceinline__ int find_job(const JobDev *__restrict__ jobs, int n_jobs, uint32_t item)
+{
+    int lo = 0, hi = n_jobs;   // last j with item_begin <= item
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(&jobs[mid].item_begin) <= item) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+constexpr int kStages = 2;
+constexpr int kWarpBuf = 64;
+
+struct WBuf {
+    longlong2 ab[kWarpBuf];
+    double d[kWarpBuf];
+    uint32_t job[kWarpBuf];
     uint32_t count;
-    unsigned long long gbase;
 };
 
-// Warp-aggregated append of this iteration's matches to the block buffer.
-__device__ __forceinline__ void emit(SBuf &sb, const MatchOut &out, bool m, long long ida, long long idb,
-                                     double dist, uint32_t job)
+// Warp-aggregated append of this iteration's matches to the warp's buffer.
+__device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, long long ida, long long idb,
+                                       double dist, uint32_t job)
 {
     const unsigned act = __activemask();
     const unsigned bal = __ballot_sync(act, m);
@@ -295,20 +314,22 @@ __device__ __forceinline__ void emit(SBuf &sb, const MatchOut &out, bool m, long
     const uint32_t n = (uint32_t)__popc(bal);
     const uint32_t rank = (uint32_t)__popc(bal & lanemask_lt());
     uint32_t base = 0;
-    if ((int)lane == leader) base = atomicAdd(&sb.count, n);
+    if ((int)lane == leader) {
+        base = wb.count;
+        wb.count = base + n;
+    }
     base = __shfl_sync(bal, base, leader);
     const uint32_t slot = base + rank;
-    if (slot < (uint32_t)kSbuf) {
-        sb.ab[slot] = make_longlong2(ida, idb);
-        sb.d[slot] = dist;
-        sb.job[slot] = job;
+    if (slot < (uint32_t)kWarpBuf) {
+        wb.ab[slot] = make_longlong2(ida, idb);
+        wb.d[slot] = dist;
+        wb.job[slot] = job;
     }
-    if (base + n <= (uint32_t)kSbuf) return;
-    // block buffer full: the lanes past its end append straight to global memory
-    const uint32_t keep = base >= (uint32_t)kSbuf ? 0u : (uint32_t)kSbuf - base;
+    if (base + n <= (uint32_t)kWarpBuf) return;
+    const uint32_t keep = base >= (uint32_t)kWarpBuf ? 0u : (uint32_t)kWarpBuf - base;
     unsigned over = bal;
     for (uint32_t q = 0; q < keep; ++q) over &= over - 1;
-    if (slot < (uint32_t)kSbuf) return;
+    if (slot < (uint32_t)kWarpBuf) return;
     const int l2 = __ffs(over) - 1;
     unsigned long long g = 0;
     if ((int)lane == l2) g = atomicAdd(&out.counters[0], (unsigned long long)__popc(over));
@@ -321,38 +342,30 @@ __device__ __forceinline__ void emit(SBuf &sb, const MatchOut &out, bool m, long
     }
 }
 
-__device__ __forceinline__ void flush(SBuf &sb, const MatchOut &out)
+// Whole warp (converged): one atomicAdd, then a coalesced copy.
+__device__ __forceinline__ void flush_w(WBuf &wb, const MatchOut &out)
 {
-    __syncthreads();
-    const uint32_t n = sb.count < (uint32_t)kSbuf ? sb.count : (uint32_t)kSbuf;
-    if (threadIdx.x == 0) sb.gbase = n ? atomicAdd(&out.counters[0], (unsigned long long)n) : 0ull;
-    __syncthreads();
-    const unsigned long long g = sb.gbase;
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+    __syncwarp();
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t n = wb.count < (uint32_t)kWarpBuf ? wb.count : (uint32_t)kWarpBuf;
+    unsigned long long g = 0;
+    if (lane == 0 && n) g = atomicAdd(&out.counters[0], (unsigned long long)n);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    for (uint32_t k = lane; k < n; k += 32) {
         if (g + k < out.cap) {
-            reinterpret_cast<longlong2 *>(out.pairs)[g + k] = sb.ab[k];
-            if (out.dist) out.dist[g + k] = sb.d[k];
-            if (out.job) out.job[g + k] = sb.job[k];
+            reinterpret_cast<longlong2 *>(out.pairs)[g + k] = wb.ab[k];
+            if (out.dist) out.dist[g + k] = wb.d[k];
+            if (out.job) out.job[g + k] = wb.job[k];
         }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) sb.count = 0;
-    __syncthreads();
-}
-
-__device__ __forceinline__ int find_job(const JobDev *__restrict__ jobs, int n_jobs, uint32_t item)
-{
-    int lo = 0, hi = n_jobs;   // last j with item_begin <= item
-    while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (__ldg(&jobs[mid].item_begin) <= item) lo = mid; else hi = mid;
-    }
-    return lo;
+    __syncwarp();
+    if (lane == 0) wb.count = 0;
+    __syncwarp();
 }
 
 // All candidates of one A object against the view; emits matches.
 template <int VARIANT, bool COUNT_CAND, bool DIST>
-__device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BView &V, SBuf &sb, const MatchOut &out,
+__device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BView &V, WBuf &wb, const MatchOut &out,
                                             uint32_t jx, Counters &cn)
 {
     Cursor c;
@@ -405,252 +418,346 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
             idb = __ldg(&J.b_id[global_index(V, c.zb, q)]);
             if (DIST) dist = 2.0 * asin(sqrt(c2) * 0.5);
         }
-        emit(sb, out, m, a.id, idb, dist, jx);
+        emit_w(wb, out, m, a.id, idb, dist, jx);
     }
 }
 
-struct Stage {
-    double2 radec[kStageCap];
-    float4 xyz[kStageCap];
-    uint32_t off[kMaxSeg + 1];
-    uint32_t g[kMaxSeg];
-    uint32_t src[kMaxSeg];
-    uint64_t bar;
-    // tile descriptor (written by thread 0)
-    uint32_t t_start, t_len;
-    int t_zf, t_zl;
-    int mode;               // 0 staged, 1 global fallback
-    int band_lo, nseg;
-    uint32_t total;
-    double ra_first, ra_last;
-    // tile formation state
-    int z;                  // current zone
-    uint32_t pos;           // current A index
-    uint32_t item, item_end;
-    int z1;                 // end zone of the item
-    int jx;
-    int error;
+// ---------------------------------------------------------------------------
+// Tile plans (pre-pass, one thread per work item)
+// ---------------------------------------------------------------------------
+constexpr int kMaxBand = 72;       // B zones a staged band may span
+constexpr int kMaxPlanSeg = 4;     // per-zone windows of a UNION plan
+
+enum : uint32_t { PLAN_WHOLE = 0, PLAN_UNION = 1, PLAN_GLOBAL = 2 };
+
+struct __align__(16) TilePlan {    // 64 bytes
+    uint32_t a_start, a_len;
+    uint32_t mode, nseg;           // nseg = band zones
+    int32_t band_lo;
+    uint32_t job;
+    uint32_t b_start, b_len;       // WHOLE: the band's contiguous B range; UNION: total staged
+    uint32_t seg_g[kMaxPlanSeg];   // UNION: first staged B object of band zone k
+    uint32_t seg_len[kMaxPlanSeg];
+};
+static_assert(sizeof(TilePlan) == 64, "plan layout");
+
+// Cuts work item `item` into tiles (see the file header); calls f(start, len, zf, zl).
+template <class F>
+__device__ __forceinline__ void for_each_tile(const JobDev &J, uint32_t item, uint32_t zc, uint32_t tile, F f)
+{
+    const int z0 = J.z_lo + (int)((item - J.item_begin) * zc);
+    const int z1 = min(z0 + (int)zc, J.z_hi + 1);
+    const uint32_t *zo = J.a_zoff;
+    int z = z0;
+    uint32_t pos = zo[z0];
+    while (true) {
+        while (z < z1 && pos >= zo[z + 1]) {
+            ++z;
+            pos = max(pos, zo[z]);
+        }
+        if (z >= z1) return;
+        const uint32_t zb0 = zo[z], zb1 = zo[z + 1];
+        const uint32_t cnt = zb1 - zb0;
+        if (cnt > tile / 2) {            // large zone: near-equal single-zone tiles
+            const uint32_t k = (cnt + tile - 1) / tile;
+            const uint32_t size = (cnt + k - 1) / k;
+            const uint32_t len = min(size, zb1 - pos);
+            f(pos, len, z, z);
+            pos += len;
+        } else {                         // consecutive small zones packed together
+            const uint32_t start = pos;
+            uint32_t end = zb1;
+            int zl = z, zn = z + 1;
+            while (zn < z1) {
+                const uint32_t e1 = zo[zn + 1];
+                const uint32_t c1 = e1 - zo[zn];
+                if (c1 > tile / 2 || e1 - start > tile) break;
+                if (c1 > 0) {
+                    zl = zn;
+                    end = e1;
+                }
+                ++zn;
+            }
+            f(start, end - start, z, zl);
+            pos = end;
+            z = zn;
+        }
+    }
+}
+
+__global__ void tiles_count(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32_t zc,
+                            uint32_t tile, uint32_t *__restrict__ cnt)
+{
+    const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= n_items) return;
+    const JobDev &J = jobs[n_jobs > 1 ? find_job(jobs, n_jobs, item) : 0];
+    uint32_t c = 0;
+    for_each_tile(J, item, zc, tile, [&](uint32_t, uint32_t, int, int) { ++c; });
+    cnt[item] = c;
+}
+
+__global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32_t zc, uint32_t tile,
+                           uint32_t cap_b, const uint32_t *__restrict__ off, TilePlan *__restrict__ plans,
+                           uint32_t max_tiles, unsigned long long *err)
+{
+    const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= n_items) return;
+    const int jx = n_jobs > 1 ? find_job(jobs, n_jobs, item) : 0;
+    const JobDev &J = jobs[jx];
+    uint32_t o = off[item];
+    for_each_tile(J, item, zc, tile, [&](uint32_t start, uint32_t len, int zf, int zl) {
+        TilePlan P;
+        P.a_start = start;
+        P.a_len = len;
+        P.job = (uint32_t)jx;
+        const int band_lo = max(0, zf - J.nz), band_hi = min(J.n_zones - 1, zl + J.nz);
+        P.band_lo = band_lo;
+        P.nseg = (uint32_t)(band_hi - band_lo + 1);
+        const uint32_t B0 = J.b_zoff[band_lo], B1 = J.b_zoff[band_hi + 1];
+        P.b_start = B0;
+        P.b_len = B1 - B0;
+        P.mode = PLAN_GLOBAL;
+        for (int k = 0; k < kMaxPlanSeg; ++k) P.seg_g[k] = P.seg_len[k] = 0;
+        if ((int)P.nseg <= kMaxBand && P.b_len <= cap_b) {
+            P.mode = PLAN_WHOLE;
+        } else if (zf == zl && (int)P.nseg <= kMaxPlanSeg && J.alpha[zf] < 3.0) {
+            const double alpha = J.alpha[zf];
+            const double ra_f = J.a_radec[start].x, ra_l = J.a_radec[start + len - 1].x;
+            uint32_t total = 0;
+            for (int k = 0; k < (int)P.nseg; ++k) {
+                const uint32_t b0 = J.b_zoff[band_lo + k], b1 = J.b_zoff[band_lo + k + 1];
+                uint32_t sb = b0, ln = b1 - b0;
+                if (ln > 0) {
+                    const double bmin = J.b_radec[b0].x, bmax = J.b_radec[b1 - 1].x;
+                    const bool wrap = !((ra_l + alpha + 2 * kWinEps - XM_TWO_PI < bmin) &&
+                                        (ra_f - alpha - 2 * kWinEps + XM_TWO_PI > bmax));
+                    if (!wrap) {
+                        sb = lower_ra_g(J.b_radec, b0, b1, ra_f - alpha - kWinEps);
+                        ln = upper_ra_g(J.b_radec, sb, b1, ra_l + alpha + kWinEps) - sb;
+                    }
+                }
+                P.seg_g[k] = sb;
+                P.seg_len[k] = ln;
+                total += ln;
+            }
+            if (total <= cap_b) {
+                P.mode = PLAN_UNION;
+                P.b_len = total;
+            }
+        }
+        if (o < max_tiles) plans[o] = P;
+        else atomicExch(err, 1ull);
+        ++o;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Warp-specialised pair kernel: warp 0 produces (bulk copies into a ring of
+// stages), warps 1..C consume (one A object per thread).
+// ---------------------------------------------------------------------------
+template <int TILE>
+struct StageT {
+    static constexpr int kCapB = 4 * TILE;
+    double2 b_radec[kCapB];
+    float4 b_xyz[kCapB];
+    double2 a_radec[TILE];
+    float4 a_xyz[TILE];
+    long long a_id[TILE + 2];
+    uint32_t zoff[kMaxBand + 8];   // B zone offsets of the band (WHOLE), 16-byte aligned copy
+    // descriptor (written by the producer before the full-barrier arrive)
+    uint32_t a_start, a_len, mode, nseg;
+    int32_t band_lo;
+    uint32_t job, b_start, id_skew, zoff_skew, done;
+    uint32_t seg_off[kMaxPlanSeg + 1];
+    uint32_t seg_g[kMaxPlanSeg];
 };
 
 template <int TILE, int VARIANT, bool COUNT_CAND, bool DIST>
-__global__ void __launch_bounds__(TILE)
-pair_kernel(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32_t zc, uint32_t chunk, MatchOut out)
+__global__ void __launch_bounds__(TILE + 32)
+pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
+            const uint32_t *__restrict__ n_tiles_ptr, uint32_t max_tiles, uint32_t chunk, MatchOut out)
 {
-    __shared__ SBuf sb;
-    __shared__ __align__(128) Stage st;
-    const int tid = threadIdx.x;
-    const unsigned lane = tid & 31;
-    if (tid == 0) {
-        sb.count = 0;
-        st.error = 0;
-        mbar_init(&st.bar, 1);
+    using Stage = StageT<TILE>;
+    constexpr int C = TILE / 32;   // consumer warps
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    Stage *stages = reinterpret_cast<Stage *>(smem_raw);
+    WBuf *wbufs = reinterpret_cast<WBuf *>(stages + kStages);
+    uint64_t *full = reinterpret_cast<uint64_t *>(wbufs + C);
+    uint64_t *empty = full + kStages;
+
+    const int warp = threadIdx.x >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t n_tiles = min(*n_tiles_ptr, max_tiles);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], C);
+        }
         fence_mbar_init();
     }
+    if (warp >= 1 && lane == 0) wbufs[warp - 1].count = 0;
     __syncthreads();
-    uint32_t phase = 0;
-    Counters cn = {0ull, 0ull, 0ull, 0ull};
-    bool failed = false;
 
-    for (;;) {
-        // ---- claim `chunk` work items ----
-        if (tid == 0) {
-            const uint32_t i0 = (uint32_t)atomicAdd(&out.counters[1], (unsigned long long)chunk);
-            st.item = i0;
-            st.item_end = min(i0 + chunk, n_items);
-            st.jx = -1;
-        }
-        __syncthreads();
-        if (st.item >= n_items) break;
-        // ---- tiles of the claimed items ----
+    if (warp == 0) {
+        // ================= producer =================
+        int s = 0;
+        uint32_t phase = 0;
+        bool ok = true;
+        int issued = 0;              // stages issued and possibly in flight (for the exit drain)
         for (;;) {
-            if (tid == 0) {
-                // next tile: advance (item, zone, pos)
-                st.t_len = 0;
-                while (st.item < st.item_end) {
-                    if (st.jx < 0) {
-                        const int jx = n_jobs > 1 ? find_job(jobs, n_jobs, st.item) : 0;
-                        const JobDev &Jt = jobs[jx];
-                        st.jx = jx;
-                        st.z = Jt.z_lo + (int)((st.item - Jt.item_begin) * zc);
-                        st.z1 = min(st.z + (int)zc, Jt.z_hi + 1);
-                        st.pos = __ldg(&Jt.a_zoff[st.z]);
-                    }
-                    const JobDev &Jt = jobs[st.jx];
-                    const uint32_t *zo = Jt.a_zoff;
-                    int z = st.z;
-                    uint32_t pos = st.pos;
-                    while (z < st.z1 && pos >= __ldg(&zo[z + 1])) {
-                        ++z;
-                        pos = max(pos, __ldg(&zo[z]));
-                    }
-                    if (z >= st.z1) {   // item done
-                        st.item++;
-                        st.jx = -1;
-                        continue;
-                    }
-                    const uint32_t zb0 = __ldg(&zo[z]), zb1 = __ldg(&zo[z + 1]);
-                    const uint32_t cnt = zb1 - zb0;
-                    if (cnt > (uint32_t)(TILE / 2)) {   // large zone: near-equal single-zone tiles
-                        const uint32_t k = (cnt + TILE - 1) / TILE;
-                        const uint32_t size = (cnt + k - 1) / k;
-                        const uint32_t len = min(size, zb1 - pos);
-                        st.t_start = pos;
-                        st.t_len = len;
-                        st.t_zf = st.t_zl = z;
-                        st.pos = pos + len;
-                        st.z = z;
-                    } else {                          // pack small zones
-                        const uint32_t start = pos;
-                        uint32_t end = zb1;
-                        int zl = z, zn = z + 1;
-                        while (zn < st.z1) {
-                            const uint32_t e1 = __ldg(&zo[zn + 1]);
-                            const uint32_t c1 = e1 - __ldg(&zo[zn]);
-                            if (c1 > (uint32_t)(TILE / 2) || e1 - start > (uint32_t)TILE) break;
-                            if (c1 > 0) {
-                                zl = zn;
-                                end = e1;
-                            }
-                            ++zn;
-                        }
-                        st.t_start = start;
-                        st.t_len = end - start;
-                        st.t_zf = z;
-                        st.t_zl = zl;
-                        st.pos = end;
-                        st.z = zn;
-                    }
+            uint32_t t0 = 0;
+            if (lane == 0) t0 = (uint32_t)atomicAdd(&out.counters[1], (unsigned long long)chunk);
+            t0 = __shfl_sync(0xffffffffu, t0, 0);
+            if (t0 >= n_tiles) break;
+            const uint32_t nt = min(chunk, n_tiles - t0);
+            for (uint32_t k = 0; k < nt && ok; ++k) {
+                if (!mbar_wait(&empty[s], phase ^ 1u)) {
+                    ok = false;
                     break;
-                }
-            }
-            __syncthreads();
-            if (st.t_len == 0) break;   // claimed items exhausted
-            const JobDev &J = jobs[st.jx];
-            const uint32_t t_start = st.t_start, t_len = st.t_len;
-            const int zf = st.t_zf, zl = st.t_zl;
-            // ---- this thread's A object ----
-            AObj a;
-            const bool active = (uint32_t)tid < t_len;
-            if (active) {
-                const uint32_t i = t_start + tid;
-                const float4 fa = __ldg(&J.a_xyz[i]);
-                const double2 ra = __ldg(&J.a_radec[i]);
-                a.ra = ra.x;
-                a.dec = ra.y;
-                a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
-                a.zone = (int)__float_as_uint(fa.w);
-                a.alpha = __ldg(&J.alpha[a.zone]);
-                a.full_ring = a.alpha >= 3.0;
-                a.id = __ldg(&J.a_id[i]);
-                a.have_xyz = false;
-                if (tid == 0) st.ra_first = a.ra;
-                if ((uint32_t)tid == t_len - 1) st.ra_last = a.ra;
-            }
-            __syncthreads();
-            // ---- staging plan: warp 0 ----
-            if (tid < 32) {
-                const int band_lo = max(0, zf - J.nz), band_hi = min(J.n_zones - 1, zl + J.nz);
-                const int nseg = band_hi - band_lo + 1;
-                int mode = nseg > kMaxSeg ? 1 : 0;
-                if (mode == 0) {
-                    const bool single = zf == zl;
-                    const double alpha = __ldg(&J.alpha[zf]);
-                    const double ra_f = st.ra_first, ra_l = st.ra_last;
-                    uint32_t carry = 0;
-                    for (int k0 = 0; k0 < nseg; k0 += 32) {
-                        const int k = k0 + (int)lane;
-                        uint32_t s = 0, len = 0;
-                        if (k < nseg) {
-                            const int zb = band_lo + k;
-                            const uint32_t b0 = __ldg(&J.b_zoff[zb]), b1 = __ldg(&J.b_zoff[zb + 1]);
-                            s = b0;
-                            len = b1 - b0;
-                            if (len > 0 && single && alpha < 3.0) {
-                                const double bmin = __ldg(&J.b_radec[b0].x), bmax = __ldg(&J.b_radec[b1 - 1].x);
-                                const bool wrap = !((ra_l + alpha + 2 * kWinEps - XM_TWO_PI < bmin) &&
-                                                    (ra_f - alpha - 2 * kWinEps + XM_TWO_PI > bmax));
-                                if (!wrap) {
-                                    s = lower_ra_g(J.b_radec, b0, b1, ra_f - alpha - kWinEps);
-                                    const uint32_t e = upper_ra_g(J.b_radec, s, b1, ra_l + alpha + kWinEps);
-                                    len = e - s;
-                                }
-                            }
-                        }
-                        // exclusive scan of len across the warp
-                        uint32_t x = len;
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                            if (lane >= (unsigned)o) x += y;
-                        }
-                        if (k < nseg) {
-                            st.off[k] = carry + x - len;
-                            st.g[k] = s;
-                        }
-                        carry += __shfl_sync(0xffffffffu, x, 31);
-                    }
-                    if (lane == 0) {
-                        st.off[nseg] = carry;
-                        st.total = carry;
-                        if (carry > (uint32_t)kStageCap) mode = 1;
-                    }
                 }
                 if (lane == 0) {
-                    st.mode = mode;
-                    st.band_lo = band_lo;
-                    st.nseg = nseg;
-                }
-            }
-            __syncthreads();
-            const int mode = st.mode;
-            if (mode == 0 && st.total > 0) {
-                // ---- bulk copies of the staged windows ----
-                if (tid == 0) {
+                    const TilePlan &P = plans[t0 + k];
+                    Stage &S = stages[s];
+                    const JobDev &J = jobs[P.job];
+                    S.a_start = P.a_start;
+                    S.a_len = P.a_len;
+                    S.mode = P.mode;
+                    S.nseg = P.nseg;
+                    S.band_lo = P.band_lo;
+                    S.job = P.job;
+                    S.b_start = P.b_start;
+                    S.done = 0;
+                    const uint32_t a_even = P.a_start & ~1u;
+                    S.id_skew = P.a_start - a_even;
+                    const uint32_t id_cnt = (P.a_start + P.a_len - a_even + 1) & ~1u;
+                    uint32_t bytes = P.a_len * 32u + id_cnt * 8u;
+                    uint32_t zcopy = 0, z_al = 0;
+                    if (P.mode == PLAN_WHOLE) {
+                        bytes += P.b_len * 32u;
+                        z_al = (uint32_t)P.band_lo & ~3u;
+                        S.zoff_skew = (uint32_t)P.band_lo - z_al;
+                        zcopy = (S.zoff_skew + P.nseg + 1 + 3) & ~3u;
+                        bytes += zcopy * 4u;
+                    } else if (P.mode == PLAN_UNION) {
+                        bytes += P.b_len * 32u;
+                        uint32_t o = 0;
+                        for (uint32_t q = 0; q < P.nseg; ++q) {
+                            S.seg_off[q] = o;
+                            S.seg_g[q] = P.seg_g[q];
+                            o += P.seg_len[q];
+                        }
+                        S.seg_off[P.nseg] = o;
+                    }
                     fence_proxy_async();
-                    mbar_expect_tx(&st.bar, st.total * (uint32_t)(sizeof(double2) + sizeof(float4)));
-                    for (int k = 0; k < st.nseg; ++k) {
-                        const uint32_t o = st.off[k], len = st.off[k + 1] - o;
-                        if (len == 0) continue;
-                        bulk_g2s(&st.radec[o], J.b_radec + st.g[k], len * (uint32_t)sizeof(double2), &st.bar);
-                        bulk_g2s(&st.xyz[o], J.b_xyz + st.g[k], len * (uint32_t)sizeof(float4), &st.bar);
+                    mbar_expect_tx(&full[s], bytes);
+                    bulk_g2s(S.a_radec, J.a_radec + P.a_start, P.a_len * 16u, &full[s]);
+                    bulk_g2s(S.a_xyz, J.a_xyz + P.a_start, P.a_len * 16u, &full[s]);
+                    bulk_g2s(S.a_id, J.a_id + a_even, id_cnt * 8u, &full[s]);
+                    if (P.mode == PLAN_WHOLE) {
+                        if (P.b_len) {
+                            bulk_g2s(S.b_radec, J.b_radec + P.b_start, P.b_len * 16u, &full[s]);
+                            bulk_g2s(S.b_xyz, J.b_xyz + P.b_start, P.b_len * 16u, &full[s]);
+                        }
+                        bulk_g2s(S.zoff, J.b_zoff + z_al, zcopy * 4u, &full[s]);
+                    } else if (P.mode == PLAN_UNION) {
+                        for (uint32_t q = 0; q < P.nseg; ++q) {
+                            const uint32_t ln = P.seg_len[q];
+                            if (!ln) continue;
+                            bulk_g2s(S.b_radec + S.seg_off[q], J.b_radec + P.seg_g[q], ln * 16u, &full[s]);
+                            bulk_g2s(S.b_xyz + S.seg_off[q], J.b_xyz + P.seg_g[q], ln * 16u, &full[s]);
+                        }
                     }
                 }
-                const bool ok = mbar_wait(&st.bar, phase);
-                phase ^= 1u;
-                if (__syncthreads_or(!ok)) {
-                    // copies did not land in time: report, wait once more for them, stop
-                    if (tid == 0) {
-                        atomicExch((unsigned long long *)&out.counters[7], 1ull);
-                        mbar_wait(&st.bar, phase ^ 1u);
-                    }
-                    __syncthreads();
-                    failed = true;
-                    break;
+                __syncwarp();
+                issued++;
+                if (++s == kStages) {
+                    s = 0;
+                    phase ^= 1u;
                 }
             }
-            if (active) {
-                BView V;
-                V.staged = mode == 0;
-                if (V.staged) {
-                    V.radec = st.radec;
-                    V.xyz = st.xyz;
-                    V.off = st.off;
-                    V.g = st.g;
-                    V.band_lo = st.band_lo;
-                } else {
-                    V.radec = J.b_radec;
-                    V.xyz = J.b_xyz;
-                    V.zoff = J.b_zoff;
-                }
-                test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, sb, out, (uint32_t)st.jx, cn);
-            }
-            __syncthreads();
-            if (sb.count >= (uint32_t)(kSbuf / 2)) flush(sb, out);
+            if (!ok) break;
         }
-        if (failed) break;
-        flush(sb, out);
+        // end of work: a "done" stage for the consumers
+        if (ok && mbar_wait(&empty[s], phase ^ 1u)) {
+            if (lane == 0) {
+                stages[s].done = 1;
+                mbar_expect_tx(&full[s], 0);
+            }
+            __syncwarp();
+        } else {
+            if (lane == 0) atomicExch(&out.counters[7], 1ull);
+            // wait (bounded) for copies still landing in the stages before leaving
+            for (int q = 0; q < kStages && q < issued; ++q) {
+                if (++s == kStages) {
+                    s = 0;
+                    phase ^= 1u;
+                }
+                mbar_wait(&full[s], phase);
+            }
+        }
+        return;
     }
-    // statistics: one atomic per warp
+
+    // ================= consumers =================
+    WBuf &wb = wbufs[warp - 1];
+    Counters cn = {0ull, 0ull, 0ull, 0ull};
+    int s = 0;
+    uint32_t phase = 0;
+    for (;;) {
+        if (!mbar_wait(&full[s], phase)) {
+            if (lane == 0) atomicExch(&out.counters[7], 1ull);
+            break;
+        }
+        Stage &S = stages[s];
+        if (S.done) break;
+        const uint32_t t = (uint32_t)(warp - 1) * 32u + lane;
+        if (t < S.a_len) {
+            const JobDev &J = jobs[S.job];
+            AObj a;
+            const float4 fa = S.a_xyz[t];
+            const double2 ra = S.a_radec[t];
+            a.ra = ra.x;
+            a.dec = ra.y;
+            a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
+            a.zone = (int)__float_as_uint(fa.w);
+            a.alpha = __ldg(&J.alpha[a.zone]);
+            a.full_ring = a.alpha >= 3.0;
+            a.id = S.a_id[S.id_skew + t];
+            a.have_xyz = false;
+            BView V;
+            V.band_lo = S.band_lo;
+            if (S.mode == PLAN_WHOLE) {
+                V.staged = true;
+                V.radec = S.b_radec;
+                V.xyz = S.b_xyz;
+                V.zoff = S.zoff + S.zoff_skew;
+                V.base = S.b_start;
+                V.whole = true;
+            } else if (S.mode == PLAN_UNION) {
+                V.staged = true;
+                V.radec = S.b_radec;
+                V.xyz = S.b_xyz;
+                V.off = S.seg_off;
+                V.g = S.seg_g;
+                V.whole = false;
+            } else {
+                V.staged = false;
+                V.radec = J.b_radec;
+                V.xyz = J.b_xyz;
+                V.zoff = J.b_zoff;
+                V.whole = false;
+            }
+            test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
+        }
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[s])) : "memory");
+        if (wb.count >= (uint32_t)(kWarpBuf / 2)) flush_w(wb, out);
+        if (++s == kStages) {
+            s = 0;
+            phase ^= 1u;
+        }
+    }
+    flush_w(wb, out);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         cn.tested += __shfl_down_sync(0xffffffffu, cn.tested, o);
@@ -666,45 +773,78 @@ pair_kernel(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint3
     }
 }
 
+template <int TILE>
+constexpr size_t smem_bytes()
+{
+    return kStages * sizeof(StageT<TILE>) + (TILE / 32) * sizeof(WBuf) + 2 * kStages * sizeof(uint64_t);
+}
+
 template <int TILE, int VARIANT, bool CC, bool DIST>
-cudaError_t launch_t(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, const MatchOut &out,
-                     cudaStream_t st)
+cudaError_t launch_t(const LaunchCfg &L, const JobDev *jobs, const TilePlan *plans, const uint32_t *n_tiles,
+                     uint32_t max_tiles, const MatchOut &out, cudaStream_t st)
 {
     auto k = pair_kernel<TILE, VARIANT, CC, DIST>;
+    const size_t smem = smem_bytes<TILE>();
+    static bool attr = false;   // per instantiation
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
     int per_sm = L.blocks_per_sm;
     if (per_sm <= 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TILE, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TILE + 32, smem);
         if (per_sm < 1) per_sm = 1;
     }
-    const uint64_t want = ((uint64_t)n_items + L.chunk - 1) / L.chunk;
+    const uint64_t want = ((uint64_t)max_tiles + L.chunk - 1) / L.chunk;
     unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)L.sm_count * per_sm, std::max<uint64_t>(want, 1));
-    k<<<grid, TILE, 0, st>>>(jobs, n_jobs, n_items, L.zc, L.chunk, out);
+    k<<<grid, TILE + 32, smem, st>>>(jobs, plans, n_tiles, max_tiles, L.chunk, out);
     return cudaGetLastError();
 }
 
 template <int TILE>
-cudaError_t launch_tile(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, const MatchOut &out,
-                        cudaStream_t st)
+cudaError_t launch_tile(const LaunchCfg &L, const JobDev *jobs, const TilePlan *plans, const uint32_t *n_tiles,
+                        uint32_t max_tiles, const MatchOut &out, cudaStream_t st)
 {
     if (L.variant == 1)
-        return L.dist ? launch_t<TILE, 1, true, true>(L, jobs, n_jobs, n_items, out, st)
-                      : launch_t<TILE, 1, true, false>(L, jobs, n_jobs, n_items, out, st);
+        return L.dist ? launch_t<TILE, 1, true, true>(L, jobs, plans, n_tiles, max_tiles, out, st)
+                      : launch_t<TILE, 1, true, false>(L, jobs, plans, n_tiles, max_tiles, out, st);
     if (L.count_cand)
-        return L.dist ? launch_t<TILE, 0, true, true>(L, jobs, n_jobs, n_items, out, st)
-                      : launch_t<TILE, 0, true, false>(L, jobs, n_jobs, n_items, out, st);
-    return L.dist ? launch_t<TILE, 0, false, true>(L, jobs, n_jobs, n_items, out, st)
-                  : launch_t<TILE, 0, false, false>(L, jobs, n_jobs, n_items, out, st);
+        return L.dist ? launch_t<TILE, 0, true, true>(L, jobs, plans, n_tiles, max_tiles, out, st)
+                      : launch_t<TILE, 0, true, false>(L, jobs, plans, n_tiles, max_tiles, out, st);
+    return L.dist ? launch_t<TILE, 0, false, true>(L, jobs, plans, n_tiles, max_tiles, out, st)
+                  : launch_t<TILE, 0, false, false>(L, jobs, plans, n_tiles, max_tiles, out, st);
 }
 
 }  // namespace
 
-cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, const MatchOut &out,
-                         cudaStream_t st)
+uint64_t plan_bound(uint32_t n_items, uint64_t total_a, int tile)
 {
+    // a tile holds more than tile/2 objects unless it ends a work item or
+    // precedes a large zone (which then holds more than tile/2)
+    return (uint64_t)n_items + 2 * (4 * total_a / (uint64_t)tile + 1) + 1;
+}
+
+size_t plan_bytes(uint64_t n_plans) { return (size_t)n_plans * sizeof(TilePlan); }
+
+cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, void *plans,
+                         uint32_t *tile_cnt, uint32_t *tile_off, void *scan_tmp, uint32_t max_tiles,
+                         const MatchOut &out, cudaStream_t st)
+{
+    const unsigned g = (n_items + 127) / 128;
+    tiles_count<<<g, 128, 0, st>>>(jobs, n_jobs, n_items, L.zc, (uint32_t)L.tile, tile_cnt);
+    cudaError_t e = xm_scan_exclusive_u32(tile_cnt, tile_off, n_items, scan_tmp, st);
+    if (e != cudaSuccess) return e;
+    const uint32_t cap_b = 4u * (uint32_t)L.tile;
+    tiles_make<<<g, 128, 0, st>>>(jobs, n_jobs, n_items, L.zc, (uint32_t)L.tile, cap_b, tile_off,
+                                  (TilePlan *)plans, max_tiles, out.counters + 7);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const uint32_t *n_tiles = tile_off + n_items;
     switch (L.tile) {
-    case 64: return launch_tile<64>(L, jobs, n_jobs, n_items, out, st);
-    case 256: return launch_tile<256>(L, jobs, n_jobs, n_items, out, st);
-    default: return launch_tile<128>(L, jobs, n_jobs, n_items, out, st);
+    case 64: return launch_tile<64>(L, jobs, (const TilePlan *)plans, n_tiles, max_tiles, out, st);
+    case 256: return launch_tile<256>(L, jobs, (const TilePlan *)plans, n_tiles, max_tiles, out, st);
+    default: return launch_tile<128>(L, jobs, (const TilePlan *)plans, n_tiles, max_tiles, out, st);
     }
 }
 

@@ -45,7 +45,16 @@ struct LaunchCfg {
     bool dist = true;
 };
 
-cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items,
+// Upper bound of the number of tiles (plans) for n_items work items over
+// total_a A objects, and the bytes of that many plans.
+uint64_t plan_bound(uint32_t n_items, uint64_t total_a, int tile);
+size_t plan_bytes(uint64_t n_plans);
+
+// Tile pre-pass (count, scan, plans) and the pair kernel, all on `st`.
+// tile_cnt: [n_items], tile_off: [n_items + 1], scan_tmp: xm_scan_tmp_bytes(n_items),
+// plans: plan_bytes(max_tiles) with max_tiles >= plan_bound(...).
+cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, void *plans,
+                         uint32_t *tile_cnt, uint32_t *tile_off, void *scan_tmp, uint32_t max_tiles,
                          const MatchOut &out, cudaStream_t st);
 
 }  // namespace xm
