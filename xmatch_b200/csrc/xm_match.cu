@@ -293,7 +293,16 @@ __device__ __forceinline__ int find_job(const JobDev *__restrict__ jobs, int n_j
 }
 
 constexpr int kStages = 2;
-constexpr int kWarpBuf = 64;
+constexpr int kWarpBuf = 32;
+
+constexpr int kMaxRanges = 9;   // 3 windows x up to 3 zones per lane; beyond that the cursor path
+
+// Per-warp candidate ranges of phase 1: start | length << 16 (staged indices < 2^16).
+struct WList {
+    uint32_t r[32][kMaxRanges];
+    uint32_t pre[32];              // inclusive prefix of candidate counts
+    double alpha[32];
+};
 
 struct WBuf {
     longlong2 ab[kWarpBuf];
@@ -361,6 +370,105 @@ __device__ __forceinline__ void flush_w(WBuf &wb, const MatchOut &out)
     __syncwarp();
     if (lane == 0) wb.count = 0;
     __syncwarp();
+}
+
+// Per-tile job scalars kept in registers.
+struct JobScalars {
+    double sr_rad, sr_dist2;
+    float thr_hi, thr_lo;
+    int n_zones, nz;
+};
+
+__device__ __forceinline__ JobScalars load_scalars(const JobDev &J)
+{
+    JobScalars k;
+    k.sr_rad = J.sr_rad;
+    k.sr_dist2 = J.sr_dist2;
+    k.thr_hi = J.thr_hi;
+    k.thr_lo = J.thr_lo;
+    k.n_zones = J.n_zones;
+    k.nz = J.nz;
+    return k;
+}
+
+__device__ __forceinline__ bool cuts_k(const JobScalars &K, double ra_a, double dec_a, double alpha, double2 rb)
+{
+    if (!(fabs(__dsub_rn(dec_a, rb.y)) < K.sr_rad)) return false;
+    const double d = __dsub_rn(ra_a, rb.x);
+    return fabs(d) < alpha || fabs(__dsub_rn(d, XM_TWO_PI)) < alpha || fabs(__dadd_rn(d, XM_TWO_PI)) < alpha;
+}
+
+// first k in [lo, hi) with ra[k] > v (shared-memory view)
+__device__ __forceinline__ uint32_t upper_v(const BView &V, uint32_t lo, uint32_t hi, double v)
+{
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (V.radec[mid].x <= v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Phase 1: a lane's candidate ranges in the staged view (same sets as the
+// cursor enumeration of next_candidate).  Returns the number of candidates,
+// or -1 if the ranges do not fit the per-lane list.
+__device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, double ra, double alpha, bool full_ring,
+                                           int zone, uint32_t *rr, int &nr)
+{
+    nr = 0;
+    int total = 0;
+    const int zlo = max(0, zone - K.nz), zhi = min(K.n_zones - 1, zone + K.nz);
+    const double lo = ra - alpha - kWinEps, hi = ra + alpha + kWinEps;
+    for (int zb = zlo; zb <= zhi; ++zb) {
+        uint32_t b0, b1;
+        const int k = zb - V.band_lo;
+        if (V.whole) {
+            b0 = V.zoff[k] - V.base;
+            b1 = V.zoff[k + 1] - V.base;
+        } else {
+            b0 = V.off[k];
+            b1 = V.off[k + 1];
+        }
+        if (b0 >= b1) continue;
+        // append [s, e) to the lane's list
+#define XM_PUSH(s_, e_)                                    \
+    do {                                                   \
+        if ((e_) > (s_)) {                                 \
+            if (nr == kMaxRanges) return -1;               \
+            rr[nr++] = (s_) | (((e_) - (s_)) << 16);       \
+            total += (int)((e_) - (s_));                   \
+        }                                                  \
+    } while (0)
+        if (full_ring) {
+            XM_PUSH(b0, b1);
+        } else {
+            const uint32_t j0 = lower_v(V, b0, b1, lo);
+            const uint32_t j1 = upper_v(V, j0, b1, hi);
+            XM_PUSH(j0, j1);
+            const double hi2 = hi - XM_TWO_PI + kWinEps;
+            if (hi2 >= V.radec[b0].x) {
+                const uint32_t w0 = lower_v(V, b0, j0, lo - XM_TWO_PI - kWinEps);
+                const uint32_t w1 = upper_v(V, w0, j0, hi2);
+                XM_PUSH(w0, w1);
+            }
+            const double lo3 = lo + XM_TWO_PI - kWinEps;
+            if (lo3 <= V.radec[b1 - 1].x) {
+                const uint32_t w0 = lower_v(V, j1, b1, lo3);
+                const uint32_t w1 = upper_v(V, w0, b1, hi + XM_TWO_PI + kWinEps);
+                XM_PUSH(w0, w1);
+            }
+        }
+#undef XM_PUSH
+    }
+    return total;
+}
+
+// Staged B index -> global B index.
+__device__ __forceinline__ uint32_t staged_global(const BView &V, int nseg, uint32_t q)
+{
+    if (V.whole) return V.base + q;
+    int k = 0;
+    while (k + 1 < nseg && V.off[k + 1] <= q) ++k;
+    return V.g[k] + (q - V.off[k]);
 }
 
 // All candidates of one A object against the view; emits matches.
@@ -582,7 +690,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Stage *stages = reinterpret_cast<Stage *>(smem_raw);
     WBuf *wbufs = reinterpret_cast<WBuf *>(stages + kStages);
-    uint64_t *full = reinterpret_cast<uint64_t *>(wbufs + C);
+    WList *wl = reinterpret_cast<WList *>(wbufs + C);
+    uint64_t *full = reinterpret_cast<uint64_t *>(wl + C);
     uint64_t *empty = full + kStages;
 
     const int warp = threadIdx.x >> 5;
@@ -711,43 +820,150 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
         Stage &S = stages[s];
         if (S.done) break;
         const uint32_t t = (uint32_t)(warp - 1) * 32u + lane;
-        if (t < S.a_len) {
-            const JobDev &J = jobs[S.job];
-            AObj a;
-            const float4 fa = S.a_xyz[t];
-            const double2 ra = S.a_radec[t];
-            a.ra = ra.x;
-            a.dec = ra.y;
-            a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
-            a.zone = (int)__float_as_uint(fa.w);
-            a.alpha = __ldg(&J.alpha[a.zone]);
-            a.full_ring = a.alpha >= 3.0;
-            a.id = S.a_id[S.id_skew + t];
-            a.have_xyz = false;
-            BView V;
-            V.band_lo = S.band_lo;
-            if (S.mode == PLAN_WHOLE) {
-                V.staged = true;
-                V.radec = S.b_radec;
-                V.xyz = S.b_xyz;
-                V.zoff = S.zoff + S.zoff_skew;
-                V.base = S.b_start;
-                V.whole = true;
-            } else if (S.mode == PLAN_UNION) {
-                V.staged = true;
-                V.radec = S.b_radec;
-                V.xyz = S.b_xyz;
-                V.off = S.seg_off;
-                V.g = S.seg_g;
-                V.whole = false;
-            } else {
+        const JobDev &J = jobs[S.job];
+        const JobScalars K = load_scalars(J);
+        if (S.mode == PLAN_GLOBAL) {
+            // band too large to stage: per-lane cursor over global memory
+            if (t < S.a_len) {
+                AObj a;
+                const float4 fa = S.a_xyz[t];
+                const double2 ra = S.a_radec[t];
+                a.ra = ra.x;
+                a.dec = ra.y;
+                a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
+                a.zone = (int)__float_as_uint(fa.w);
+                a.alpha = __ldg(&J.alpha[a.zone]);
+                a.full_ring = a.alpha >= 3.0;
+                a.id = S.a_id[S.id_skew + t];
+                a.have_xyz = false;
+                BView V;
                 V.staged = false;
+                V.whole = false;
                 V.radec = J.b_radec;
                 V.xyz = J.b_xyz;
                 V.zoff = J.b_zoff;
-                V.whole = false;
+                V.band_lo = 0;
+                test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
             }
-            test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
+        } else {
+            BView V;
+            V.staged = true;
+            V.whole = S.mode == PLAN_WHOLE;
+            V.band_lo = S.band_lo;
+            V.radec = S.b_radec;
+            V.xyz = S.b_xyz;
+            V.zoff = S.zoff + S.zoff_skew;
+            V.base = S.b_start;
+            V.off = S.seg_off;
+            V.g = S.seg_g;
+            // ---- phase 1: each lane's candidate ranges ----
+            WList &L = wl[warp - 1];
+            int n = 0, nr = 0;
+            double ra_a = 0, dec_a = 0, alpha = 0;
+            if (t < S.a_len) {
+                const float4 fa = S.a_xyz[t];
+                const double2 rd = S.a_radec[t];
+                ra_a = rd.x;
+                dec_a = rd.y;
+                const int za = (int)__float_as_uint(fa.w);
+                alpha = __ldg(&J.alpha[za]);
+                n = lane_ranges(V, K, ra_a, alpha, alpha >= 3.0, za, L.r[lane], nr);
+            }
+            L.alpha[lane] = alpha;
+            const bool overflow = __any_sync(0xffffffffu, n < 0);
+            if (overflow) {
+                // a lane has more windows than the list holds (nz > 1): cursor path for this warp
+                if (t < S.a_len) {
+                    AObj a;
+                    const float4 fa = S.a_xyz[t];
+                    a.ra = ra_a;
+                    a.dec = dec_a;
+                    a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
+                    a.zone = (int)__float_as_uint(fa.w);
+                    a.alpha = alpha;
+                    a.full_ring = alpha >= 3.0;
+                    a.id = S.a_id[S.id_skew + t];
+                    a.have_xyz = false;
+                    test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
+                }
+            } else {
+                // inclusive scan of candidate counts across the warp
+                uint32_t incl = (uint32_t)n;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= (unsigned)o) incl += y;
+                }
+                L.pre[lane] = incl;
+                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                __syncwarp();
+                // ---- phase 2: the warp walks the flattened candidate list ----
+                for (uint32_t c0 = 0; c0 < total; c0 += 32) {
+                    const uint32_t c = c0 + lane;
+                    bool m = false;
+                    long long ida = 0, idb = 0;
+                    double dist = 0;
+                    if (c < total) {
+                        // owner lane: first lane whose inclusive prefix exceeds c
+                        int lo = 0, hi = 31;
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if (L.pre[mid] > c) hi = mid; else lo = mid + 1;
+                        }
+                        const int owner = lo;
+                        uint32_t k = c - (owner ? L.pre[owner - 1] : 0u);
+                        int r = 0;
+                        uint32_t rr = L.r[owner][0];
+                        while (k >= (rr >> 16)) {
+                            k -= rr >> 16;
+                            rr = L.r[owner][++r];
+                        }
+                        const uint32_t q = (rr & 0xFFFFu) + k;
+                        const uint32_t ta = (warp - 1) * 32u + (uint32_t)owner;
+                        cn.tested++;
+                        const double2 ra = S.a_radec[ta];
+                        const double2 rb = S.b_radec[q];
+                        const double al = L.alpha[owner];
+                        double c2 = 0;
+                        if (VARIANT == 0) {
+                            if (COUNT_CAND) cn.cand += cuts_k(K, ra.x, ra.y, al, rb) ? 1ull : 0ull;
+                            const float4 fa = S.a_xyz[ta];
+                            const float4 fb = S.b_xyz[q];
+                            const float dx = fa.x - fb.x, dy = fa.y - fb.y, dz = fa.z - fb.z;
+                            const float c32 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            if (!(c32 > K.thr_hi)) {
+                                cn.border += (c32 >= K.thr_lo) ? 1ull : 0ull;
+                                cn.exact++;
+                                if (cuts_k(K, ra.x, ra.y, al, rb)) {
+                                    double x1, y1, z1, x2, y2, z2;
+                                    radec2xyz(ra.x, ra.y, x1, y1, z1);
+                                    radec2xyz(rb.x, rb.y, x2, y2, z2);
+                                    c2 = chord2(x1, y1, z1, x2, y2, z2);
+                                    m = c2 < K.sr_dist2;
+                                }
+                            }
+                        } else {
+                            if (cuts_k(K, ra.x, ra.y, al, rb)) {
+                                cn.cand++;
+                                cn.exact++;
+                                double x1, y1, z1, x2, y2, z2;
+                                radec2xyz(ra.x, ra.y, x1, y1, z1);
+                                radec2xyz(rb.x, rb.y, x2, y2, z2);
+                                c2 = chord2(x1, y1, z1, x2, y2, z2);
+                                m = c2 < K.sr_dist2;
+                            }
+                        }
+                        if (m) {
+                            ida = S.a_id[S.id_skew + ta];
+                            idb = __ldg(&J.b_id[staged_global(V, (int)S.nseg, q)]);
+                            if (DIST) dist = 2.0 * asin(sqrt(c2) * 0.5);
+                        }
+                    }
+                    emit_w(wb, out, m, ida, idb, dist, S.job);
+                    __syncwarp();
+                    if (wb.count >= (uint32_t)(kWarpBuf / 2)) flush_w(wb, out);
+                }
+            }
         }
         __syncwarp();
         if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[s])) : "memory");
@@ -776,7 +992,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
 template <int TILE>
 constexpr size_t smem_bytes()
 {
-    return kStages * sizeof(StageT<TILE>) + (TILE / 32) * sizeof(WBuf) + 2 * kStages * sizeof(uint64_t);
+    return kStages * sizeof(StageT<TILE>) + (TILE / 32) * (sizeof(WBuf) + sizeof(WList)) +
+           2 * kStages * sizeof(uint64_t);
 }
 
 template <int TILE, int VARIANT, bool CC, bool DIST>
