@@ -86,12 +86,12 @@ typedef struct xm_stats {
     float ms_zb_count, ms_zb_scan, ms_zb_scatter, ms_zb_sort;
 } xm_stats;
 
-/* Tuning of the persistent pair kernel (0 = default / autotuned).  The work
- * list holds items of `zones` consecutive A zones; a block claims `chunk`
- * items at a time and cuts them into tiles of at most `tile` objects. */
+/* Tuning of the persistent pair kernel (0 = default / autotuned).  A work
+ * item of `zones` consecutive A zones is cut into tiles of at most `tile`
+ * objects; a block claims `chunk` tiles at a time. */
 typedef struct xm_tuning {
-    uint32_t tile;        /* A objects per tile (= threads per block): 64, 128, 256 */
-    uint32_t chunk;       /* work items claimed per work-stealing step */
+    uint32_t tile;        /* A objects per tile (= consumer threads per block): 64, 128, 256 */
+    uint32_t chunk;       /* tiles claimed per work-stealing step (1..32) */
     uint32_t blocks_per_sm;
     uint32_t zones;       /* zones per work item (1..64) */
 } xm_tuning;

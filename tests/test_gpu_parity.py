@@ -155,7 +155,7 @@ def test_duplicate_coordinates(ctx):
     check_parity(ctx, A, A, 1, variants=(0,))
 
 
-@pytest.mark.parametrize("tile,chunk,zones", [(64, 1, 1), (128, 4, 16), (256, 2, 64)])
+@pytest.mark.parametrize("tile,chunk,zones", [(64, 1, 1), (128, 16, 16), (256, 32, 64)])
 def test_tuning_does_not_change_results(ctx, fixtures, tile, chunk, zones):
     a, _ = fixtures
     check_parity(ctx, a, a, 5, variants=(0,), tuning=(tile, chunk, 0, zones))

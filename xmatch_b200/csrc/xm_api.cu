@@ -501,7 +501,7 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         if (tuning->zones) L.zc = tuning->zones;
     }
     if (L.tile != 64 && L.tile != 128 && L.tile != 256) return XM_ERR_INVALID;
-    if (L.zc < 1 || L.zc > 64 || L.chunk < 1) return XM_ERR_INVALID;
+    if (L.zc < 1 || L.zc > 64 || L.chunk < 1 || L.chunk > 32) return XM_ERR_INVALID;
     Prepared P;
     XM_TRY(prepare_jobs(ctx, jobs, n_jobs, L.zc, P));
     size_t jb = P.jobs.size() * sizeof(xm::JobDev);

@@ -203,14 +203,14 @@ extern "C" xm_status xm_autotune_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t
     if (!ctx || !best || (n_jobs && !jobs)) return XM_ERR_INVALID;
     cudaSetDevice(ctx->device);
     const uint32_t tiles[] = {64, 128, 256};
-    const uint32_t chunks[] = {1, 4};
+    const uint32_t chunks[] = {4, 16};
     const uint32_t zones[] = {4, 16, 64};
     float bms = 1e30f;
-    xm_tuning b = {128, 2, 0, 16};
+    xm_tuning b = {128, 16, 0, 16};
     float fixed = 0;
-    // fixed-tile reference point: tile 128, 16 zones per item, 2 items per claim
+    // fixed-tile reference point: tile 128, 16 zones per item, 16 tiles per claim
     {
-        xm_tuning t = {128, 2, 0, 16};
+        xm_tuning t = {128, 16, 0, 16};
         float ms = 0;
         XM_TRY(xm_run_jobs(ctx, jobs, n_jobs, flags, &t, n_jobs > 1, nullptr, &ms));   // warm (and size the output)
         XM_TRY(xm_run_jobs(ctx, jobs, n_jobs, flags, &t, n_jobs > 1, nullptr, &ms));

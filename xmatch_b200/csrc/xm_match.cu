@@ -681,7 +681,7 @@ struct StageT {
 };
 
 template <int TILE, int VARIANT, bool COUNT_CAND, bool DIST>
-__global__ void __launch_bounds__(TILE + 32)
+__global__ void __launch_bounds__(TILE + 32, TILE <= 128 ? 4 : 2)
 pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             const uint32_t *__restrict__ n_tiles_ptr, uint32_t max_tiles, uint32_t chunk, MatchOut out)
 {
@@ -709,71 +709,106 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
 
     if (warp == 0) {
         // ================= producer =================
+        // Claims `chunk` (<= 32) tiles at a time; lane k prefetches plan k of
+        // the claim, lane 0 issues the copies.  The next claim is requested
+        // before the current one is issued, so its latency overlaps.
         int s = 0;
         uint32_t phase = 0;
         bool ok = true;
-        int issued = 0;              // stages issued and possibly in flight (for the exit drain)
-        for (;;) {
-            uint32_t t0 = 0;
-            if (lane == 0) t0 = (uint32_t)atomicAdd(&out.counters[1], (unsigned long long)chunk);
-            t0 = __shfl_sync(0xffffffffu, t0, 0);
-            if (t0 >= n_tiles) break;
-            const uint32_t nt = min(chunk, n_tiles - t0);
-            for (uint32_t k = 0; k < nt && ok; ++k) {
+        int issued = 0;
+        const uint32_t ch = min(chunk, 32u);
+        uint32_t t0 = 0;
+        if (lane == 0) t0 = (uint32_t)atomicAdd(&out.counters[1], (unsigned long long)ch);
+        t0 = __shfl_sync(0xffffffffu, t0, 0);
+        int cached_job = -1;
+        const double2 *a_radec = nullptr, *b_radec = nullptr;
+        const float4 *a_xyz = nullptr, *b_xyz = nullptr;
+        const long long *a_id = nullptr;
+        const uint32_t *b_zoff = nullptr;
+        while (ok && t0 < n_tiles) {
+            const uint32_t nt = min(ch, n_tiles - t0);
+            uint4 pw[4];
+            if (lane < nt) {
+                const uint4 *src = reinterpret_cast<const uint4 *>(plans + t0 + lane);
+                pw[0] = src[0]; pw[1] = src[1]; pw[2] = src[2]; pw[3] = src[3];
+            }
+            uint32_t t_next = 0;
+            if (lane == 0) t_next = (uint32_t)atomicAdd(&out.counters[1], (unsigned long long)ch);
+            for (uint32_t k = 0; k < nt; ++k) {
+                // plan k from lane k
+                uint32_t w[16];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    w[4 * q + 0] = __shfl_sync(0xffffffffu, pw[q].x, k);
+                    w[4 * q + 1] = __shfl_sync(0xffffffffu, pw[q].y, k);
+                    w[4 * q + 2] = __shfl_sync(0xffffffffu, pw[q].z, k);
+                    w[4 * q + 3] = __shfl_sync(0xffffffffu, pw[q].w, k);
+                }
                 if (!mbar_wait(&empty[s], phase ^ 1u)) {
                     ok = false;
                     break;
                 }
                 if (lane == 0) {
-                    const TilePlan &P = plans[t0 + k];
+                    const uint32_t a_start = w[0], a_len = w[1], mode = w[2], nseg = w[3];
+                    const int band_lo = (int)w[4];
+                    const uint32_t job = w[5], b_start = w[6], b_len = w[7];
+                    if ((int)job != cached_job) {
+                        const JobDev &J = jobs[job];
+                        a_radec = J.a_radec; a_xyz = J.a_xyz; a_id = J.a_id;
+                        b_radec = J.b_radec; b_xyz = J.b_xyz; b_zoff = J.b_zoff;
+                        cached_job = (int)job;
+                    }
                     Stage &S = stages[s];
-                    const JobDev &J = jobs[P.job];
-                    S.a_start = P.a_start;
-                    S.a_len = P.a_len;
-                    S.mode = P.mode;
-                    S.nseg = P.nseg;
-                    S.band_lo = P.band_lo;
-                    S.job = P.job;
-                    S.b_start = P.b_start;
+                    S.a_start = a_start;
+                    S.a_len = a_len;
+                    S.mode = mode;
+                    S.nseg = nseg;
+                    S.band_lo = band_lo;
+                    S.job = job;
+                    S.b_start = b_start;
                     S.done = 0;
-                    const uint32_t a_even = P.a_start & ~1u;
-                    S.id_skew = P.a_start - a_even;
-                    const uint32_t id_cnt = (P.a_start + P.a_len - a_even + 1) & ~1u;
-                    uint32_t bytes = P.a_len * 32u + id_cnt * 8u;
+                    const uint32_t a_even = a_start & ~1u;
+                    S.id_skew = a_start - a_even;
+                    const uint32_t id_cnt = (a_start + a_len - a_even + 1) & ~1u;
+                    uint32_t bytes = a_len * 32u + id_cnt * 8u;
                     uint32_t zcopy = 0, z_al = 0;
-                    if (P.mode == PLAN_WHOLE) {
-                        bytes += P.b_len * 32u;
-                        z_al = (uint32_t)P.band_lo & ~3u;
-                        S.zoff_skew = (uint32_t)P.band_lo - z_al;
-                        zcopy = (S.zoff_skew + P.nseg + 1 + 3) & ~3u;
+                    if (mode == PLAN_WHOLE) {
+                        bytes += b_len * 32u;
+                        z_al = (uint32_t)band_lo & ~3u;
+                        S.zoff_skew = (uint32_t)band_lo - z_al;
+                        zcopy = (S.zoff_skew + nseg + 1 + 3) & ~3u;
                         bytes += zcopy * 4u;
-                    } else if (P.mode == PLAN_UNION) {
-                        bytes += P.b_len * 32u;
+                    } else if (mode == PLAN_UNION) {
+                        bytes += b_len * 32u;
                         uint32_t o = 0;
-                        for (uint32_t q = 0; q < P.nseg; ++q) {
-                            S.seg_off[q] = o;
-                            S.seg_g[q] = P.seg_g[q];
-                            o += P.seg_len[q];
+#pragma unroll
+                        for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
+                            if (q < nseg) {
+                                S.seg_off[q] = o;
+                                S.seg_g[q] = w[8 + q];
+                                o += w[12 + q];
+                            }
                         }
-                        S.seg_off[P.nseg] = o;
+                        S.seg_off[nseg] = o;
                     }
                     fence_proxy_async();
                     mbar_expect_tx(&full[s], bytes);
-                    bulk_g2s(S.a_radec, J.a_radec + P.a_start, P.a_len * 16u, &full[s]);
-                    bulk_g2s(S.a_xyz, J.a_xyz + P.a_start, P.a_len * 16u, &full[s]);
-                    bulk_g2s(S.a_id, J.a_id + a_even, id_cnt * 8u, &full[s]);
-                    if (P.mode == PLAN_WHOLE) {
-                        if (P.b_len) {
-                            bulk_g2s(S.b_radec, J.b_radec + P.b_start, P.b_len * 16u, &full[s]);
-                            bulk_g2s(S.b_xyz, J.b_xyz + P.b_start, P.b_len * 16u, &full[s]);
+                    bulk_g2s(S.a_radec, a_radec + a_start, a_len * 16u, &full[s]);
+                    bulk_g2s(S.a_xyz, a_xyz + a_start, a_len * 16u, &full[s]);
+                    bulk_g2s(S.a_id, a_id + a_even, id_cnt * 8u, &full[s]);
+                    if (mode == PLAN_WHOLE) {
+                        if (b_len) {
+                            bulk_g2s(S.b_radec, b_radec + b_start, b_len * 16u, &full[s]);
+                            bulk_g2s(S.b_xyz, b_xyz + b_start, b_len * 16u, &full[s]);
                         }
-                        bulk_g2s(S.zoff, J.b_zoff + z_al, zcopy * 4u, &full[s]);
-                    } else if (P.mode == PLAN_UNION) {
-                        for (uint32_t q = 0; q < P.nseg; ++q) {
-                            const uint32_t ln = P.seg_len[q];
-                            if (!ln) continue;
-                            bulk_g2s(S.b_radec + S.seg_off[q], J.b_radec + P.seg_g[q], ln * 16u, &full[s]);
-                            bulk_g2s(S.b_xyz + S.seg_off[q], J.b_xyz + P.seg_g[q], ln * 16u, &full[s]);
+                        bulk_g2s(S.zoff, b_zoff + z_al, zcopy * 4u, &full[s]);
+                    } else if (mode == PLAN_UNION) {
+#pragma unroll
+                        for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
+                            const uint32_t ln = w[12 + q];
+                            if (q >= nseg || !ln) continue;
+                            bulk_g2s(S.b_radec + S.seg_off[q], b_radec + w[8 + q], ln * 16u, &full[s]);
+                            bulk_g2s(S.b_xyz + S.seg_off[q], b_xyz + w[8 + q], ln * 16u, &full[s]);
                         }
                     }
                 }
@@ -784,7 +819,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     phase ^= 1u;
                 }
             }
-            if (!ok) break;
+            t0 = __shfl_sync(0xffffffffu, t_next, 0);
         }
         // end of work: a "done" stage for the consumers
         if (ok && mbar_wait(&empty[s], phase ^ 1u)) {

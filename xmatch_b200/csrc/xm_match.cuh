@@ -37,7 +37,7 @@ struct MatchOut {
 struct LaunchCfg {
     int tile = 128;            // A objects per tile = threads per block
     uint32_t zc = 16;          // zones per work item
-    uint32_t chunk = 2;        // work items per work-stealing claim
+    uint32_t chunk = 16;       // tiles per work-stealing claim (<= 32)
     int blocks_per_sm = 0;     // 0 = occupancy limit
     int sm_count = 148;
     int variant = 0;           // 0 FP32 reject + FP64 decision, 1 plain FP64
