@@ -472,21 +472,71 @@ void or_alpha_table(double sr_deg, double zh_deg, int64_t n_zones, double *out)
     for (int64_t z = 0; z < n_zones; ++z) out[z] = or_calc_alpha_zone(sr_deg, zh_deg, (int)z);
 }
 
-/* sorted segment export: id, ra/dec radians, zone begin/end (Segment.h:36-38) */
+/* ------------------------------------------------------------------ */
+/* segment order of the GPU zone builder (for export comparisons)      */
+/* ------------------------------------------------------------------ */
+/* quantised ra: floor(ra_rad * 2^31/pi), clamped to [0, 2^32-1] */
+static inline uint32_t or_raq32(double ra_rad)
+{
+    double x = floor(ra_rad * 0x1.45f306dc9c883p+29);
+    if (!(x > 0.0)) return 0u;
+    if (x >= 4294967295.0) return 0xFFFFFFFFu;
+    return (uint32_t)x;
+}
+
+/* raq bits kept in the sort key: whole 8-bit digits, >= 28 raq bits, <= 32 */
+int or_raq_bits(int64_t n_zones)
+{
+    int zb = 0;
+    for (uint64_t v = (uint64_t)n_zones; v; v >>= 1) ++zb;
+    int p = (zb + 28 + 7) / 8;
+    int rb = 8 * p - zb;
+    return rb < 32 ? rb : 32;
+}
+
+typedef struct {
+    uint64_t key;   /* zone << raq_bits | raq */
+    int64_t idx;
+} or_qkey;
+
+static int or_qkey_cmp(const void *pa, const void *pb)
+{
+    const or_qkey *a = (const or_qkey *)pa, *b = (const or_qkey *)pb;
+    if (a->key != b->key) return a->key < b->key ? -1 : 1;
+    return a->idx < b->idx ? -1 : (a->idx > b->idx);
+}
+
+/* Sorted segment as the GPU builder lays it out: ordered by (zone, leading
+ * raq bits, input index); id, ra/dec radians, zone begin/end
+ * (Segment.h:36-38).  Returns the number of objects kept. */
 int64_t or_build_export(const or_obj *o, int64_t n, double zh_deg, int64_t *id, double *radec,
                         int64_t *zbeg, int64_t *zend, int64_t zcap)
 {
-    or_seg s;
-    if (or_seg_build(&s, o, n, zh_deg)) return -1;
-    for (int64_t i = 0; i < s.n; ++i) {
-        if (id) id[i] = s.id[i];
-        if (radec) { radec[2 * i] = s.ra[i]; radec[2 * i + 1] = s.dec[i]; }
+    int64_t n_zones = (int64_t)ceil(180 / zh_deg);
+    int rb = or_raq_bits(n_zones);
+    or_qkey *k = (or_qkey *)malloc(sizeof(or_qkey) * (size_t)(n > 0 ? n : 1));
+    if (!k) return -1;
+    int64_t m = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t z = or_zone_id(o[i].dec, zh_deg, n_zones);
+        if (z < 0 || !isfinite(o[i].ra)) continue;
+        double ra = o[i].ra / OR_RAD2DEG;
+        k[m].key = ((uint64_t)z << rb) | (uint64_t)(or_raq32(ra) >> (32 - rb));
+        k[m].idx = i;
+        ++m;
     }
-    for (int64_t z = 0; z < s.n_zones && z < zcap; ++z) {
-        if (zbeg) zbeg[z] = s.zbeg[z];
-        if (zend) zend[z] = s.zend[z];
+    qsort(k, (size_t)m, sizeof(or_qkey), or_qkey_cmp);
+    for (int64_t j = 0; j < m; ++j) {
+        const or_obj *p = &o[k[j].idx];
+        if (id) id[j] = p->id;
+        if (radec) { radec[2 * j] = p->ra / OR_RAD2DEG; radec[2 * j + 1] = p->dec / OR_RAD2DEG; }
     }
-    int64_t m = s.n;
-    or_seg_free(&s);
+    int64_t j = 0;
+    for (int64_t z = 0; z < n_zones && z < zcap; ++z) {
+        if (zbeg) zbeg[z] = j;
+        while (j < m && (int64_t)(k[j].key >> rb) == z) ++j;
+        if (zend) zend[z] = j;
+    }
+    free(k);
     return m;
 }

@@ -356,9 +356,6 @@ extern "C" xm_status xm_segment_free(xm_segment *seg)
     xm_dev_free(ctx, seg->radec);
     xm_dev_free(ctx, seg->xyz);
     xm_dev_free(ctx, seg->tmp);
-    xm_dev_free(ctx, seg->cnt);
-    xm_dev_free(ctx, seg->scan_tmp);
-    xm_dev_free(ctx, seg->big);
     delete seg;
     return XM_OK;
 }
@@ -464,6 +461,7 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
         d.nz = p.nz;
         d.z_lo = A->z_lo;
         d.z_hi = A->z_hi;
+        d.raq_shift = 32 - B->raq_bits;
         d.nA = (uint32_t)A->n;
         d.item_begin = (uint32_t)items;
         if (A->n > 0 && B->n > 0 && A->z_hi >= A->z_lo) {

@@ -59,19 +59,16 @@ struct xm_segment {
     double zh_deg = 0;
     int32_t n_zones = 0;
     int32_t z_lo = 0, z_hi = -1;   // first / last zone holding an object
+    int raq_bits = 32;             // leading bits of the quantised ra kept in xyz.w
+    uint32_t dropped_host = 0;
     uint32_t *zone_off = nullptr;  // [n_zones + 8]; [n_zones + 1] = dropped count; the rest
                                    // pads 16-byte bulk copies of zone-offset slices
     int64_t *id = nullptr;
     double2 *radec = nullptr;      // radians
     float4 *xyz = nullptr;         // FP32 unit vector; w = zone id bits
     // scratch kept for rebuilds
-    void *tmp = nullptr;           // 32-byte staging records
+    void *tmp = nullptr;           // radix-sort scratch
     size_t tmp_bytes = 0;
-    uint32_t *cnt = nullptr;       // [n_zones + 4]: histogram, dropped, -, min zone, max zone
-    void *scan_tmp = nullptr;
-    size_t scan_tmp_bytes = 0;
-    uint32_t *big = nullptr;       // oversize chunk list
-    size_t big_cap = 0;
 };
 
 // ---- error plumbing ----
@@ -103,6 +100,8 @@ cudaError_t xm_scan_exclusive_u32(const uint32_t *in, uint32_t *out, size_t n, v
                                   cudaStream_t s);
 
 xm_status xm_build_impl(xm_segment *seg, const xm_obj *dev_objs, uint64_t n, xm_stats *st);
+// Sort-key layout of a segment with n_zones zones: raq bits kept, radix passes.
+void xm_raq_layout(int32_t n_zones, int *raq_bits, int *passes);
 
 // Match parameters derived on the host (Worker.cu:310-317).
 struct xm_match_params {

@@ -117,24 +117,48 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
     return false;
 }
 
-// ---- ra bisection ----
-// first k in [lo, hi) with ra[k] >= v   (global memory)
-__device__ __forceinline__ uint32_t lower_ra_g(const double2 *__restrict__ radec, uint32_t lo, uint32_t hi, double v)
+// ---- bisection on the quantised ra (xyz.w) ----
+__device__ __forceinline__ uint32_t raq_at(const float4 *xyz, uint32_t k) { return __float_as_uint(xyz[k].w); }
+__device__ __forceinline__ uint32_t raq_at_g(const float4 *xyz, uint32_t k) { return __float_as_uint(__ldg(&xyz[k].w)); }
+
+// first k in [lo, hi) with raq[k] >= t   (global memory)
+__device__ __forceinline__ uint32_t lower_raq_g(const float4 *__restrict__ xyz, uint32_t lo, uint32_t hi, uint32_t t)
 {
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(&radec[mid].x) < v) lo = mid + 1; else hi = mid;
+        if (raq_at_g(xyz, mid) < t) lo = mid + 1; else hi = mid;
     }
     return lo;
 }
-// first k in [lo, hi) with ra[k] > v    (global memory)
-__device__ __forceinline__ uint32_t upper_ra_g(const double2 *__restrict__ radec, uint32_t lo, uint32_t hi, double v)
+// first k in [lo, hi) with raq[k] > t    (global memory)
+__device__ __forceinline__ uint32_t upper_raq_g(const float4 *__restrict__ xyz, uint32_t lo, uint32_t hi, uint32_t t)
 {
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(&radec[mid].x) <= v) lo = mid + 1; else hi = mid;
+        if (raq_at_g(xyz, mid) <= t) lo = mid + 1; else hi = mid;
     }
     return lo;
+}
+
+// Window bounds of one A object in quantised-ra space: any B with ra in the
+// FP64 window has raq in [t_lo, t_hi] (raq is monotone in ra).
+struct Win {
+    uint32_t lo, hi;     // direct window
+    uint32_t lo2, hi2;   // branch 2 (B near 0)
+    uint32_t lo3, hi3;   // branch 3 (B near 2 pi)
+};
+
+__device__ __forceinline__ Win make_win(double ra, double alpha, int shift)
+{
+    const double lo = ra - alpha - kWinEps, hi = ra + alpha + kWinEps;
+    Win w;
+    w.lo = xm::raq32(lo) >> shift;
+    w.hi = xm::raq32(hi) >> shift;
+    w.lo2 = xm::raq32(lo - XM_TWO_PI - kWinEps) >> shift;
+    w.hi2 = xm::raq32(hi - XM_TWO_PI + kWinEps) >> shift;
+    w.lo3 = xm::raq32(lo + XM_TWO_PI - kWinEps) >> shift;
+    w.hi3 = xm::raq32(hi + XM_TWO_PI + kWinEps) >> shift;
+    return w;
 }
 
 // A source (a thread's object).
@@ -147,6 +171,7 @@ struct AObj {
     int zone;
     bool full_ring;     // alpha >= 3: every object of a zone is a candidate
     bool have_xyz;
+    Win w;              // quantised windows
 };
 
 // View of B for window enumeration.
@@ -172,15 +197,24 @@ struct Cursor {
     int win;                // 0 direct, 1 branch 2, 2 branch 3
     uint32_t j, j_end;      // candidate positions (view indices) of the current window
     uint32_t b0, b1;        // current zone range (view indices)
-    double hi_cur;
+    uint32_t hi_cur;        // raq upper end of the current window
     uint32_t w1_lo, w1_hi;  // direct window (keeps the wrapped ones disjoint from it)
 };
 
-__device__ __forceinline__ uint32_t lower_v(const BView &V, uint32_t lo, uint32_t hi, double v)
+__device__ __forceinline__ uint32_t lower_v(const BView &V, uint32_t lo, uint32_t hi, uint32_t t)
 {
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        if (V.radec[mid].x < v) lo = mid + 1; else hi = mid;
+        if (raq_at(V.xyz, mid) < t) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t upper_v(const BView &V, uint32_t lo, uint32_t hi, uint32_t t)
+{
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (raq_at(V.xyz, mid) <= t) lo = mid + 1; else hi = mid;
     }
     return lo;
 }
@@ -192,33 +226,29 @@ __device__ __forceinline__ void open_window(const BView &V, const AObj &a, Curso
         if (c.win != 0) return;
         c.j = c.b0;
         c.j_end = c.b1;
-        c.hi_cur = INFINITY;
+        c.hi_cur = 0xFFFFFFFFu;
         return;
     }
-    const double lo = a.ra - a.alpha - kWinEps, hi = a.ra + a.alpha + kWinEps;
     if (c.win == 0) {
-        c.j = lower_v(V, c.b0, c.b1, lo);
+        c.j = lower_v(V, c.b0, c.b1, a.w.lo);
         c.j_end = c.b1;
-        c.hi_cur = hi;
+        c.hi_cur = a.w.hi;
         c.w1_lo = c.j;
         c.w1_hi = c.j;
         return;
     }
-    if (c.win == 1) {   // branch 2: ra_b in (ra_a - 2pi - alpha, ra_a - 2pi + alpha)
-        const double hi2 = hi - XM_TWO_PI + kWinEps;
-        if (hi2 < V.radec[c.b0].x) return;
-        c.j = lower_v(V, c.b0, c.b1, lo - XM_TWO_PI - kWinEps);
+    if (c.win == 1) {   // branch 2: below the direct window
+        if (a.w.hi2 < raq_at(V.xyz, c.b0)) return;
+        c.j = lower_v(V, c.b0, c.w1_lo, a.w.lo2);
         c.j_end = c.w1_lo;
-        c.hi_cur = hi2;
+        c.hi_cur = a.w.hi2;
         return;
     }
-    // branch 3: ra_b in (ra_a + 2pi - alpha, ra_a + 2pi + alpha)
-    const double lo3 = lo + XM_TWO_PI - kWinEps;
-    if (lo3 > V.radec[c.b1 - 1].x) return;
-    const uint32_t s = lower_v(V, c.b0, c.b1, lo3);
-    c.j = s > c.w1_hi ? s : c.w1_hi;
+    // branch 3: above the direct window
+    if (a.w.lo3 > raq_at(V.xyz, c.b1 - 1)) return;
+    c.j = lower_v(V, c.w1_hi, c.b1, a.w.lo3);
     c.j_end = c.b1;
-    c.hi_cur = hi + XM_TWO_PI + kWinEps;
+    c.hi_cur = a.w.hi3;
 }
 
 __device__ __forceinline__ bool next_candidate(const BView &V, const AObj &a, Cursor &c, uint32_t &out)
@@ -226,7 +256,7 @@ __device__ __forceinline__ bool next_candidate(const BView &V, const AObj &a, Cu
     for (;;) {
         if (c.j < c.j_end) {
             const uint32_t j = c.j;
-            if (V.radec[j].x <= c.hi_cur) {
+            if (raq_at(V.xyz, j) <= c.hi_cur) {
                 c.j = j + 1;
                 if (c.win == 0) c.w1_hi = c.j;
                 out = j;
@@ -377,6 +407,7 @@ struct JobScalars {
     double sr_rad, sr_dist2;
     float thr_hi, thr_lo;
     int n_zones, nz;
+    int raq_shift;
 };
 
 __device__ __forceinline__ JobScalars load_scalars(const JobDev &J)
@@ -388,6 +419,7 @@ __device__ __forceinline__ JobScalars load_scalars(const JobDev &J)
     k.thr_lo = J.thr_lo;
     k.n_zones = J.n_zones;
     k.nz = J.nz;
+    k.raq_shift = J.raq_shift;
     return k;
 }
 
@@ -411,13 +443,12 @@ __device__ __forceinline__ uint32_t upper_v(const BView &V, uint32_t lo, uint32_
 // Phase 1: a lane's candidate ranges in the staged view (same sets as the
 // cursor enumeration of next_candidate).  Returns the number of candidates,
 // or -1 if the ranges do not fit the per-lane list.
-__device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, double ra, double alpha, bool full_ring,
+__device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, const Win &w, bool full_ring,
                                            int zone, uint32_t *rr, int &nr)
 {
     nr = 0;
     int total = 0;
     const int zlo = max(0, zone - K.nz), zhi = min(K.n_zones - 1, zone + K.nz);
-    const double lo = ra - alpha - kWinEps, hi = ra + alpha + kWinEps;
     for (int zb = zlo; zb <= zhi; ++zb) {
         uint32_t b0, b1;
         const int k = zb - V.band_lo;
@@ -441,19 +472,17 @@ __device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, 
         if (full_ring) {
             XM_PUSH(b0, b1);
         } else {
-            const uint32_t j0 = lower_v(V, b0, b1, lo);
-            const uint32_t j1 = upper_v(V, j0, b1, hi);
+            const uint32_t j0 = lower_v(V, b0, b1, w.lo);
+            const uint32_t j1 = upper_v(V, j0, b1, w.hi);
             XM_PUSH(j0, j1);
-            const double hi2 = hi - XM_TWO_PI + kWinEps;
-            if (hi2 >= V.radec[b0].x) {
-                const uint32_t w0 = lower_v(V, b0, j0, lo - XM_TWO_PI - kWinEps);
-                const uint32_t w1 = upper_v(V, w0, j0, hi2);
+            if (w.hi2 >= raq_at(V.xyz, b0)) {
+                const uint32_t w0 = lower_v(V, b0, j0, w.lo2);
+                const uint32_t w1 = upper_v(V, w0, j0, w.hi2);
                 XM_PUSH(w0, w1);
             }
-            const double lo3 = lo + XM_TWO_PI - kWinEps;
-            if (lo3 <= V.radec[b1 - 1].x) {
-                const uint32_t w0 = lower_v(V, j1, b1, lo3);
-                const uint32_t w1 = upper_v(V, w0, b1, hi + XM_TWO_PI + kWinEps);
+            if (w.lo3 <= raq_at(V.xyz, b1 - 1)) {
+                const uint32_t w0 = lower_v(V, j1, b1, w.lo3);
+                const uint32_t w1 = upper_v(V, w0, b1, w.hi3);
                 XM_PUSH(w0, w1);
             }
         }
@@ -476,6 +505,7 @@ template <int VARIANT, bool COUNT_CAND, bool DIST>
 __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BView &V, WBuf &wb, const MatchOut &out,
                                             uint32_t jx, Counters &cn)
 {
+    a.w = make_win(a.ra, a.alpha, J.raq_shift);
     Cursor c;
     c.zb = max(0, a.zone - J.nz) - 1;
     c.zb_end = min(J.n_zones - 1, a.zone + J.nz);
@@ -630,18 +660,24 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
             P.mode = PLAN_WHOLE;
         } else if (zf == zl && (int)P.nseg <= kMaxPlanSeg && J.alpha[zf] < 3.0) {
             const double alpha = J.alpha[zf];
-            const double ra_f = J.a_radec[start].x, ra_l = J.a_radec[start + len - 1].x;
+            // A is ordered by raq: every tile object's ra is within one raq step q of
+            // [ra_first, ra_last]; widen by 2q
+            const double q2 = 2.0 * ldexp(XM_TWO_PI, J.raq_shift - 32);
+            const double ra_f = J.a_radec[start].x - q2, ra_l = J.a_radec[start + len - 1].x + q2;
+            const int sh = J.raq_shift;
+            const uint32_t t_lo = xm::raq32(ra_f - alpha - kWinEps) >> sh;
+            const uint32_t t_hi = xm::raq32(ra_l + alpha + kWinEps) >> sh;
+            const uint32_t t_hi2 = xm::raq32(ra_l + alpha + 2 * kWinEps - XM_TWO_PI) >> sh;
+            const uint32_t t_lo3 = xm::raq32(ra_f - alpha - 2 * kWinEps + XM_TWO_PI) >> sh;
             uint32_t total = 0;
             for (int k = 0; k < (int)P.nseg; ++k) {
                 const uint32_t b0 = J.b_zoff[band_lo + k], b1 = J.b_zoff[band_lo + k + 1];
                 uint32_t sb = b0, ln = b1 - b0;
                 if (ln > 0) {
-                    const double bmin = J.b_radec[b0].x, bmax = J.b_radec[b1 - 1].x;
-                    const bool wrap = !((ra_l + alpha + 2 * kWinEps - XM_TWO_PI < bmin) &&
-                                        (ra_f - alpha - 2 * kWinEps + XM_TWO_PI > bmax));
+                    const bool wrap = !(t_hi2 < raq_at_g(J.b_xyz, b0) && t_lo3 > raq_at_g(J.b_xyz, b1 - 1));
                     if (!wrap) {
-                        sb = lower_ra_g(J.b_radec, b0, b1, ra_f - alpha - kWinEps);
-                        ln = upper_ra_g(J.b_radec, sb, b1, ra_l + alpha + kWinEps) - sb;
+                        sb = lower_raq_g(J.b_xyz, b0, b1, t_lo);
+                        ln = upper_raq_g(J.b_xyz, sb, b1, t_hi) - sb;
                     }
                 }
                 P.seg_g[k] = sb;
@@ -902,7 +938,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 dec_a = rd.y;
                 const int za = (int)__float_as_uint(fa.w);
                 alpha = __ldg(&J.alpha[za]);
-                n = lane_ranges(V, K, ra_a, alpha, alpha >= 3.0, za, L.r[lane], nr);
+                const Win wn = make_win(ra_a, alpha, K.raq_shift);
+                n = lane_ranges(V, K, wn, alpha >= 3.0, za, L.r[lane], nr);
             }
             L.alpha[lane] = alpha;
             const bool overflow = __any_sync(0xffffffffu, n < 0);

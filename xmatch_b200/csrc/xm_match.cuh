@@ -22,6 +22,8 @@ struct JobDev {
     int z_lo, z_hi;            // populated zone range of A
     uint32_t nA;               // objects of A
     uint32_t item_begin;       // first global work item of this job
+    int raq_shift;             // xyz.w holds raq32(ra) >> raq_shift
+    int pad;
 };
 
 struct MatchOut {

@@ -108,6 +108,17 @@ __device__ __forceinline__ int zone_of(double dec_deg, double zh_deg, int n_zone
     return (int)zd;
 }
 
+// Quantised ra: floor(ra_rad * 2^31 / pi), i.e. 2^32 steps per turn, clamped
+// to [0, 2^32 - 1] (NaN and negative values map to 0).  Monotone in ra.
+#define XM_RAQ_SCALE 0x1.45f306dc9c883p+29
+__device__ __forceinline__ uint32_t raq32(double ra_rad)
+{
+    const double x = floor(__dmul_rn(ra_rad, XM_RAQ_SCALE));
+    if (!(x > 0.0)) return 0u;
+    if (x >= 4294967295.0) return 0xFFFFFFFFu;
+    return (uint32_t)x;
+}
+
 // Order-preserving map of a double to uint64 (negative values flipped).
 __device__ __forceinline__ unsigned long long order_key(double v)
 {
