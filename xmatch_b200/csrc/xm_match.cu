@@ -430,16 +430,6 @@ __device__ __forceinline__ bool cuts_k(const JobScalars &K, double ra_a, double 
     return fabs(d) < alpha || fabs(__dsub_rn(d, XM_TWO_PI)) < alpha || fabs(__dadd_rn(d, XM_TWO_PI)) < alpha;
 }
 
-// first k in [lo, hi) with ra[k] > v (shared-memory view)
-__device__ __forceinline__ uint32_t upper_v(const BView &V, uint32_t lo, uint32_t hi, double v)
-{
-    while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (V.radec[mid].x <= v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
 // Phase 1: a lane's candidate ranges in the staged view (same sets as the
 // cursor enumeration of next_candidate).  Returns the number of candidates,
 // or -1 if the ranges do not fit the per-lane list.
@@ -489,6 +479,19 @@ __device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, 
 #undef XM_PUSH
     }
     return total;
+}
+
+// Zone of A object i of a tile spanning zones [zf, zl] (A zone offsets in
+// global memory); -1 if the offsets disagree (never for a consistent segment).
+__device__ __forceinline__ int a_zone(const uint32_t *__restrict__ a_zoff, int zf, int zl, uint32_t i)
+{
+    if (zf == zl) return zf;
+    int lo = zf, hi = zl;   // last z with a_zoff[z] <= i
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&a_zoff[mid]) <= i) lo = mid; else hi = mid - 1;
+    }
+    return (__ldg(&a_zoff[lo]) <= i && i < __ldg(&a_zoff[lo + 1])) ? lo : -1;
 }
 
 // Staged B index -> global B index.
@@ -570,7 +573,8 @@ enum : uint32_t { PLAN_WHOLE = 0, PLAN_UNION = 1, PLAN_GLOBAL = 2 };
 
 struct __align__(16) TilePlan {    // 64 bytes
     uint32_t a_start, a_len;
-    uint32_t mode, nseg;           // nseg = band zones
+    uint32_t mode;                 // mode | nseg << 8 | (zl - zf) << 16 (nseg = band zones)
+    int32_t zf;                    // first A zone of the tile
     int32_t band_lo;
     uint32_t job;
     uint32_t b_start, b_len;       // WHOLE: the band's contiguous B range; UNION: total staged
@@ -650,15 +654,16 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
         P.job = (uint32_t)jx;
         const int band_lo = max(0, zf - J.nz), band_hi = min(J.n_zones - 1, zl + J.nz);
         P.band_lo = band_lo;
-        P.nseg = (uint32_t)(band_hi - band_lo + 1);
+        P.zf = zf;
+        const uint32_t nseg = (uint32_t)(band_hi - band_lo + 1);
         const uint32_t B0 = J.b_zoff[band_lo], B1 = J.b_zoff[band_hi + 1];
         P.b_start = B0;
         P.b_len = B1 - B0;
-        P.mode = PLAN_GLOBAL;
+        uint32_t mode = PLAN_GLOBAL;
         for (int k = 0; k < kMaxPlanSeg; ++k) P.seg_g[k] = P.seg_len[k] = 0;
-        if ((int)P.nseg <= kMaxBand && P.b_len <= cap_b) {
-            P.mode = PLAN_WHOLE;
-        } else if (zf == zl && (int)P.nseg <= kMaxPlanSeg && J.alpha[zf] < 3.0) {
+        if ((int)nseg <= kMaxBand && P.b_len <= cap_b) {
+            mode = PLAN_WHOLE;
+        } else if (zf == zl && (int)nseg <= kMaxPlanSeg && J.alpha[zf] < 3.0) {
             const double alpha = J.alpha[zf];
             // A is ordered by raq: every tile object's ra is within one raq step q of
             // [ra_first, ra_last]; widen by 2q
@@ -670,7 +675,7 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
             const uint32_t t_hi2 = xm::raq32(ra_l + alpha + 2 * kWinEps - XM_TWO_PI) >> sh;
             const uint32_t t_lo3 = xm::raq32(ra_f - alpha - 2 * kWinEps + XM_TWO_PI) >> sh;
             uint32_t total = 0;
-            for (int k = 0; k < (int)P.nseg; ++k) {
+            for (int k = 0; k < (int)nseg; ++k) {
                 const uint32_t b0 = J.b_zoff[band_lo + k], b1 = J.b_zoff[band_lo + k + 1];
                 uint32_t sb = b0, ln = b1 - b0;
                 if (ln > 0) {
@@ -685,10 +690,12 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
                 total += ln;
             }
             if (total <= cap_b) {
-                P.mode = PLAN_UNION;
+                mode = PLAN_UNION;
                 P.b_len = total;
             }
         }
+        // nseg is only read for WHOLE (<= kMaxBand) and UNION (<= kMaxPlanSeg) plans
+        P.mode = mode | (min(nseg, 255u) << 8) | ((uint32_t)(zl - zf) << 16);
         if (o < max_tiles) plans[o] = P;
         else atomicExch(err, 1ull);
         ++o;
@@ -710,7 +717,7 @@ struct StageT {
     uint32_t zoff[kMaxBand + 8];   // B zone offsets of the band (WHOLE), 16-byte aligned copy
     // descriptor (written by the producer before the full-barrier arrive)
     uint32_t a_start, a_len, mode, nseg;
-    int32_t band_lo;
+    int32_t band_lo, zf, zl;
     uint32_t job, b_start, id_skew, zoff_skew, done;
     uint32_t seg_off[kMaxPlanSeg + 1];
     uint32_t seg_g[kMaxPlanSeg];
@@ -785,7 +792,9 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     break;
                 }
                 if (lane == 0) {
-                    const uint32_t a_start = w[0], a_len = w[1], mode = w[2], nseg = w[3];
+                    const uint32_t a_start = w[0], a_len = w[1], mode = w[2] & 255u, nseg = (w[2] >> 8) & 255u;
+                    const int zf = (int)w[3];
+                    const int zl = zf + (int)(w[2] >> 16);
                     const int band_lo = (int)w[4];
                     const uint32_t job = w[5], b_start = w[6], b_len = w[7];
                     if ((int)job != cached_job) {
@@ -800,6 +809,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     S.mode = mode;
                     S.nseg = nseg;
                     S.band_lo = band_lo;
+                    S.zf = zf;
+                    S.zl = zl;
                     S.job = job;
                     S.b_start = b_start;
                     S.done = 0;
@@ -902,8 +913,14 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 a.ra = ra.x;
                 a.dec = ra.y;
                 a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
-                a.zone = (int)__float_as_uint(fa.w);
-                a.alpha = __ldg(&J.alpha[a.zone]);
+                a.zone = a_zone(J.a_zoff, S.zf, S.zl, S.a_start + t);
+                if (a.zone < 0 || a.zone >= K.n_zones) {
+                    atomicExch(&out.counters[7], 1ull);
+                    a.zone = 0;
+                    a.alpha = -1.0;   // empty windows, no candidates
+                } else {
+                    a.alpha = __ldg(&J.alpha[a.zone]);
+                }
                 a.full_ring = a.alpha >= 3.0;
                 a.id = S.a_id[S.id_skew + t];
                 a.have_xyz = false;
@@ -929,15 +946,20 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             V.g = S.seg_g;
             // ---- phase 1: each lane's candidate ranges ----
             WList &L = wl[warp - 1];
-            int n = 0, nr = 0;
+            int n = 0, nr = 0, za = 0;
             double ra_a = 0, dec_a = 0, alpha = 0;
             if (t < S.a_len) {
-                const float4 fa = S.a_xyz[t];
                 const double2 rd = S.a_radec[t];
                 ra_a = rd.x;
                 dec_a = rd.y;
-                const int za = (int)__float_as_uint(fa.w);
-                alpha = __ldg(&J.alpha[za]);
+                za = a_zone(J.a_zoff, S.zf, S.zl, S.a_start + t);
+                if (za < 0 || za >= K.n_zones) {
+                    atomicExch(&out.counters[7], 1ull);
+                    za = 0;
+                    alpha = -1.0;
+                } else {
+                    alpha = __ldg(&J.alpha[za]);
+                }
                 const Win wn = make_win(ra_a, alpha, K.raq_shift);
                 n = lane_ranges(V, K, wn, alpha >= 3.0, za, L.r[lane], nr);
             }
@@ -951,7 +973,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     a.ra = ra_a;
                     a.dec = dec_a;
                     a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
-                    a.zone = (int)__float_as_uint(fa.w);
+                    a.zone = za;
                     a.alpha = alpha;
                     a.full_ring = alpha >= 3.0;
                     a.id = S.a_id[S.id_skew + t];
