@@ -34,7 +34,8 @@ enum {
     XM_ERR_NODEVICE = 6,     /* no usable CUDA device */
     XM_ERR_IO = 7,           /* file could not be read or written */
     XM_ERR_BUSY = 8,         /* serving queue full / request not finished */
-    XM_ERR_TIMEOUT = 9       /* a bounded wait ran out */
+    XM_ERR_TIMEOUT = 9,      /* a bounded wait ran out */
+    XM_ERR_TOO_LARGE = 10    /* input exceeds a fixed capacity (xm_segment_build_noalloc) */
 };
 
 /* One .idradec record: 24 bytes, little endian (Obj.h:21-25). */
@@ -168,6 +169,35 @@ xm_status xm_idradec_write(const char *path, const xm_obj *objs, uint64_t n);
 /* Append pairs to a file: mode 16 = reference records {idA, idB};
  * mode 24 = {idA, idB, dist}; mode 0 = ASCII "idA idB dist\n". */
 xm_status xm_pairs_write(const char *path, const xm_pairs *pairs, int mode, int append);
+
+/* ---- zone build without any allocation ----
+ * No counterpart in the reference.  For callers that may not allocate
+ * device memory once they are running: a serving process that reserved its
+ * HBM budget at start-up, or a host application whose device memory is owned
+ * by another allocator.  Same result as xm_segment_build_device +
+ * xm_segment_export (same sorted order), written to caller-owned device
+ * arrays; the sort scratch is a fixed array inside the library
+ * (XM_NOALLOC_MAX_OBJS records, about 25 MB of device memory, held by every
+ * GPU that loads the library until the process exits).  Calls no cudaMalloc
+ * or cudaFree and allocates nothing on the host heap.
+ *   device        GPU to run on (made current for the call)
+ *   stream        cudaStream_t to queue on (NULL = default stream); the call
+ *                 returns after the work on it has completed
+ *   dev_objs      n records in device memory, n <= XM_NOALLOC_MAX_OBJS,
+ *                 larger n returns XM_ERR_TOO_LARGE
+ *   out_id        int64  [n]      (first *n_kept used)
+ *   out_radec     double [2 n]    ra, dec radians
+ *   out_xyz       float  [4 n]    FP32 unit vector, w = quantised-ra bits
+ *   out_zone_off  uint32 [n_zones + 1], n_zones = ceil(180 / zh_deg), given
+ *                 in zone_off_cap; zone z holds [out_zone_off[z], out_zone_off[z+1])
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call uses the same scratch: calls that overlap on the GPU (from
+ * several host threads or streams) race, so serialise them per device. */
+#define XM_NOALLOC_MAX_OBJS (1u << 20)
+xm_status xm_segment_build_noalloc(int device, void *stream, const xm_obj *dev_objs, uint64_t n,
+                                   double zh_deg, int64_t *out_id, double *out_radec, float *out_xyz,
+                                   uint32_t *out_zone_off, uint64_t zone_off_cap, uint64_t *n_kept);
 
 /* ---- utilities ---- */
 /* FP64 unit vectors of (ra, dec) in degrees computed on the GPU exactly as

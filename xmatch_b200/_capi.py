@@ -20,6 +20,8 @@ XM_ERR_NODEVICE = 6
 XM_ERR_IO = 7
 XM_ERR_BUSY = 8
 XM_ERR_TIMEOUT = 9
+XM_ERR_TOO_LARGE = 10
+XM_NOALLOC_MAX_OBJS = 1 << 20
 
 XM_FILTER32 = 0
 XM_PLAIN64 = 1 << 0
@@ -95,6 +97,8 @@ SIGNATURES = {
     "xm_idradec_write": (ctypes.c_int, [ctypes.c_char_p, P, U64]),
     "xm_pairs_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(XmPairs), ctypes.c_int, ctypes.c_int]),
     "xm_unit_vectors": (ctypes.c_int, [P, P, P, U64, P]),
+    "xm_segment_build_noalloc": (ctypes.c_int, [ctypes.c_int, P, P, U64, D, P, P, P, P, U64,
+                                                ctypes.POINTER(U64)]),
     "xm_alpha_table": (ctypes.c_int, [D, D, P, I32]),
 }
 

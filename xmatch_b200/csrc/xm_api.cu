@@ -138,6 +138,7 @@ extern "C" const char *xm_status_str(xm_status s)
     case XM_ERR_IO: return "I/O error";
     case XM_ERR_BUSY: return "busy";
     case XM_ERR_TIMEOUT: return "timed out";
+    case XM_ERR_TOO_LARGE: return "input exceeds the fixed capacity of the call";
     default: return "unknown status";
     }
 }

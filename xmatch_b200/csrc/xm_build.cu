@@ -29,6 +29,8 @@
 //   3. zb_gather   SoA in sorted order, unit vectors by the project sincos
 //   4. zb_bounds   zone offsets from the sorted keys
 #include <algorithm>
+#include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "xm_internal.h"
@@ -457,5 +459,117 @@ xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stat
         stats->ms_build += a + b + c + d;
         stats->n_launches += launches;
     }
+    return XM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Zone build without allocation (xm_segment_build_noalloc).  The radix-sort
+// scratch is this file-scope device array; host code must not use its name
+// as a pointer (it is a host-side stand-in), so its device address is looked
+// up once per device with cudaGetSymbolAddress.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kNaMax = XM_NOALLOC_MAX_OBJS;
+constexpr uint64_t kNaTiles = (kNaMax + kTile - 1) / kTile;
+constexpr size_t kNaAlign(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t kNaKeys = kNaAlign(kNaMax * 8);
+constexpr size_t kNaVals = kNaAlign(kNaMax * 4);
+constexpr size_t kNaCnt = kNaAlign(kNaTiles * 256 * 4 + 4);
+constexpr size_t kNaScan = kNaAlign(((kNaTiles * 256 + 4095) / 4096 + 1) * 4);
+constexpr size_t kNaHist = kNaAlign(kMaxPasses * 256 * 4 + 64);
+constexpr size_t kNaBytes = 2 * kNaKeys + 2 * kNaVals + 2 * kNaCnt + kNaScan + kNaHist;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+constexpr int kNaMaxDevices = 64;
+void *g_noalloc_ptr[kNaMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+}  // namespace
+
+extern "C" xm_status xm_segment_build_noalloc(int device, void *stream, const xm_obj *objs, uint64_t n,
+                                              double zh_deg, int64_t *out_id, double *out_radec, float *out_xyz,
+                                              uint32_t *out_zone_off, uint64_t zone_off_cap, uint64_t *n_kept)
+{
+    if (n > kNaMax) return XM_ERR_TOO_LARGE;
+    if (!(zh_deg > 0) || !std::isfinite(zh_deg) || !out_zone_off || !n_kept || device < 0 ||
+        device >= kNaMaxDevices)
+        return XM_ERR_INVALID;
+    if (n && (!objs || !out_id || !out_radec || !out_xyz)) return XM_ERR_INVALID;
+    const double nzd = std::ceil(180 / zh_deg);
+    if (nzd > 2.0e9) return XM_ERR_INVALID;
+    const int nz = (int)nzd;
+    if (zone_off_cap < (uint64_t)nz + 1) return XM_ERR_INVALID;
+    int raq_bits, passes;
+    xm_raq_layout(nz, &raq_bits, &passes);
+    if (passes > kMaxPasses) return XM_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return XM_ERR_CUDA;
+    // one-time set-up per device: device address of the scratch array
+    void *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[device]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return XM_ERR_CUDA;
+            }
+            g_noalloc_ptr[device] = p;
+        }
+        base = g_noalloc_ptr[device];
+    }
+    int sm_count = 0;
+    if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return XM_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    char *w = (char *)base;
+    unsigned long long *k0 = (unsigned long long *)w; w += kNaKeys;
+    unsigned long long *k1 = (unsigned long long *)w; w += kNaKeys;
+    uint32_t *v0 = (uint32_t *)w; w += kNaVals;
+    uint32_t *v1 = (uint32_t *)w; w += kNaVals;
+    uint32_t *tcnt = (uint32_t *)w; w += kNaCnt;
+    uint32_t *toff = (uint32_t *)w; w += kNaCnt;
+    void *scan_tmp = w; w += kNaScan;
+    uint32_t *hist = (uint32_t *)w;
+    uint32_t *misc = hist + kMaxPasses * 256;
+    const uint32_t n_tiles = (uint32_t)((std::max<uint64_t>(n, 1) + kTile - 1) / kTile);
+    // the scratch keeps the previous call's contents: clear what accumulates
+    if (cudaMemsetAsync(hist, 0, kMaxPasses * 256 * 4 + 64, st) != cudaSuccess ||
+        cudaMemsetAsync(misc, 0xFF, 4, st) != cudaSuccess)
+        return XM_ERR_CUDA;
+    KeyParams kp{zh_deg, nz, 32 - raq_bits, raq_bits, passes};
+    if (n > 0) zb_keys<<<grid_for(n, 256, sm_count, 4), 256, 0, st>>>(objs, n, kp, k0, v0, hist, misc);
+    uint32_t h[kMaxPasses * 256 + 16];
+    if (cudaMemcpyAsync(h, hist, sizeof(uint32_t) * (kMaxPasses * 256 + 16), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return XM_ERR_CUDA;
+    const uint64_t dropped = n ? h[kMaxPasses * 256 + 2] : 0;
+    const size_t ds_smem = (size_t)kTile * 12 + (size_t)kRsWarps * 256 * 4 + 512 * 4;
+    if (cudaFuncSetAttribute(rs_downsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ds_smem) != cudaSuccess)
+        return XM_ERR_CUDA;
+    unsigned long long *kin = k0, *kout = k1;
+    uint32_t *vin = v0, *vout = v1;
+    for (int p = 0; p < passes && n > 0; ++p) {
+        bool constant = false;
+        for (int d = 0; d < 256; ++d)
+            if (h[p * 256 + d] == n) constant = true;
+        if (constant) continue;
+        rs_upsweep<<<n_tiles, kRsThreads, 0, st>>>(kin, n, 8 * p, n_tiles, tcnt);
+        if (xm_scan_exclusive_u32(tcnt, toff, (size_t)n_tiles * 256, scan_tmp, st) != cudaSuccess) return XM_ERR_CUDA;
+        rs_downsweep<<<n_tiles, kRsThreads, ds_smem, st>>>(kin, vin, n, 8 * p, n_tiles, toff, kout, vout);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    const uint64_t kept = n - dropped;
+    if (kept > 0)
+        zb_gather<<<grid_for(kept, 256, sm_count, 8), 256, 0, st>>>(kin, vin, objs, kept, (1ull << raq_bits) - 1,
+                                                                    (long long *)out_id, (double2 *)out_radec,
+                                                                    (float4 *)out_xyz);
+    if (cudaMemsetAsync(out_zone_off, 0xFF, ((size_t)nz + 1) * 4, st) != cudaSuccess) return XM_ERR_CUDA;
+    if (n > 0) zb_bounds_mark<<<grid_for(n, 256, sm_count, 8), 256, 0, st>>>(kin, n, raq_bits, nz, out_zone_off);
+    zb_bounds_fill<<<grid_for((uint64_t)nz + 1, 256, sm_count, 8), 256, 0, st>>>(kin, n, raq_bits, nz, out_zone_off);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) return XM_ERR_CUDA;
+    *n_kept = kept;
     return XM_OK;
 }
