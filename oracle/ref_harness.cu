@@ -13,9 +13,17 @@
 //
 // The kernel's block compaction (Worker.cu:157-233) also reads the shared
 // slots of threads that left at Worker.cu:125 (outside the zone ranges), so
-// a partial block can append a pair that was never tested.  With `validate`
-// set, the harness synchronises after every launch and counts, instead of
-// keeping, appended pairs that fall outside that launch's index ranges.
+// a partial block compacts stale shared memory: it drops tested matches and
+// appends pairs that were never tested.  Two modes:
+//   pad = 0  the reference launch geometry; with `validate` the harness
+//            synchronises after every launch and counts appended pairs that
+//            fall outside that launch's index ranges (evidence of the defect);
+//   pad = 1  every launch covers whole 16x16 blocks: the index ranges are
+//            extended to multiples of 16 (into the next zone's objects, or 16
+//            dummy records appended to each array that can never match), so
+//            no thread leaves early and the compaction is sound; only pairs
+//            inside the true ranges are kept.  This is the reference
+//            predicate evaluated by the reference's own code.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -58,7 +66,7 @@ extern "C" {
 long long ref_xmatch(const double *radec_a, long long na, const int *zbeg_a, const int *zend_a,
                      const double *radec_b, long long nb, const int *zbeg_b, const int *zend_b, int n_zones,
                      double sr_deg, double zh_deg, unsigned int *pairs, unsigned int cap, int *launches,
-                     int validate, long long *outside)
+                     int validate, long long *outside, int pad)
 {
     using namespace xmatch;
     dbl2 *da = nullptr, *db = nullptr;
@@ -69,13 +77,24 @@ long long ref_xmatch(const double *radec_a, long long na, const int *zbeg_a, con
     unsigned int kept = 0;
     long long out_n = 0;
     bool failed = false;
-    if (cudaMalloc(&da, sizeof(dbl2) * (na > 0 ? na : 1)) != cudaSuccess) return -1;
-    if (cudaMalloc(&db, sizeof(dbl2) * (nb > 0 ? nb : 1)) != cudaSuccess) { cudaFree(da); return -1; }
+    const long long padn = 16;   // dummy records after each array
+    if (cudaMalloc(&da, sizeof(dbl2) * (na + padn)) != cudaSuccess) return -1;
+    if (cudaMalloc(&db, sizeof(dbl2) * (nb + padn)) != cudaSuccess) { cudaFree(da); return -1; }
     if (cudaMalloc(&dm, sizeof(uint2) * (cap > 0 ? cap : 1)) != cudaSuccess) { cudaFree(da); cudaFree(db); return -1; }
     if (cudaMalloc(&dn, sizeof(unsigned int)) != cudaSuccess) { cudaFree(da); cudaFree(db); cudaFree(dm); return -1; }
     do {
         if (na && cudaMemcpy(da, radec_a, sizeof(dbl2) * na, cudaMemcpyHostToDevice) != cudaSuccess) break;
         if (nb && cudaMemcpy(db, radec_b, sizeof(dbl2) * nb, cudaMemcpyHostToDevice) != cudaSuccess) break;
+        {   // dummies: dec far outside [-pi/2, pi/2] and of opposite sign in A and B, so no pair
+            // involving one passes the dec cut of Worker.cu:88
+            dbl2 dummy_a[16], dummy_b[16];
+            for (int q = 0; q < 16; ++q) {
+                dummy_a[q].x = 0.0; dummy_a[q].y = 1000.0;
+                dummy_b[q].x = 0.0; dummy_b[q].y = -1000.0;
+            }
+            if (cudaMemcpy(da + na, dummy_a, sizeof(dummy_a), cudaMemcpyHostToDevice) != cudaSuccess) break;
+            if (cudaMemcpy(db + nb, dummy_b, sizeof(dummy_b), cudaMemcpyHostToDevice) != cudaSuccess) break;
+        }
         if (cudaMemset(dn, 0, sizeof(unsigned int)) != cudaSuccess) break;
         // Worker.cu:310-317
         const int nz = (int)ceil(sr_deg / zh_deg);
@@ -94,7 +113,10 @@ long long ref_xmatch(const double *radec_a, long long na, const int *zbeg_a, con
                 const double alpha_rad = calc_alpha(sr_deg, zh_deg, zid1);
                 dim3 dimBlock(16, 256 / 16);
                 dim3 dimGrid((n1 + dimBlock.x - 1) / dimBlock.x, (n2 + dimBlock.y - 1) / dimBlock.y);
-                xmatch_kernel<<<dimGrid, dimBlock>>>(da, i1s, i1e, db, i2s, i2e, sr_rad, alpha_rad, sr_dist2,
+                // padded ranges end on a block edge (at most 15 past the zone, within the dummies)
+                const int e1 = pad ? i1s + (int)(dimGrid.x * dimBlock.x) : i1e;
+                const int e2 = pad ? i2s + (int)(dimGrid.y * dimBlock.y) : i2e;
+                xmatch_kernel<<<dimGrid, dimBlock>>>(da, i1s, e1, db, i2s, e2, sr_rad, alpha_rad, sr_dist2,
                                                      validate ? dm + kept : dm, validate ? cap - kept : cap, dn);
                 ++nl;
                 if (validate) {

@@ -26,7 +26,7 @@ def lib():
         L.ref_xmatch.restype = ctypes.c_longlong
         L.ref_xmatch.argtypes = [P, ctypes.c_longlong, P, P, P, ctypes.c_longlong, P, P, ctypes.c_int,
                                  ctypes.c_double, ctypes.c_double, P, ctypes.c_uint, ctypes.POINTER(ctypes.c_int),
-                                 ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+                                 ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
         _lib = L
     return _lib
 
@@ -50,8 +50,13 @@ def _zone_layout(objs, zh_deg, n_zones):
     return idx, np.ascontiguousarray(radec), zb, ze
 
 
-def xmatch(A, B, sr_deg, zh_deg=None, validate=True):
-    """Pairs (idA, idB) the reference kernel appends; returns (pairs, n_outside, launches)."""
+def xmatch(A, B, sr_deg, zh_deg=None, validate=True, pad=True):
+    """Pairs (idA, idB) the reference kernel appends; returns (pairs, n_outside, launches).
+
+    pad=True launches whole 16x16 blocks only (the compaction of Worker.cu:
+    157-233 is unsound in partial blocks) and keeps the pairs inside the true
+    zone ranges: the reference predicate evaluated by its own kernel.
+    pad=False uses the reference launch geometry as is."""
     if zh_deg is None:
         zh_deg = sr_deg
     n_zones = int(np.ceil(180 / zh_deg))       # Sorter.cu:156
@@ -65,7 +70,8 @@ def xmatch(A, B, sr_deg, zh_deg=None, validate=True):
         outside = ctypes.c_longlong()
         n = L.ref_xmatch(ra.ctypes.data, len(ia), zba.ctypes.data, zea.ctypes.data, rb.ctypes.data, len(ib),
                          zbb.ctypes.data, zeb.ctypes.data, n_zones, sr_deg, zh_deg, out.ctypes.data, cap,
-                         ctypes.byref(launches), 1 if validate else 0, ctypes.byref(outside))
+                         ctypes.byref(launches), 1 if (validate or pad) else 0, ctypes.byref(outside),
+                         1 if pad else 0)
         if n < 0:
             if cap >= 1 << 30:
                 raise RuntimeError("reference kernel harness failed")
