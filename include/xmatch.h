@@ -83,8 +83,10 @@ typedef struct xm_stats {
     float ms_match;        /* device time of the pair kernel alone */
     float ms_build;        /* zone build (xm_segment_build*) */
     float ms_h2d, ms_d2h;
-    /* zone-build passes: histogram, scan, scatter into zones, sort + SoA write */
+    /* zone-build passes: sort keys + digit histograms, histogram read-back,
+       radix passes, gather into zone order + zone bounds */
     float ms_zb_count, ms_zb_scan, ms_zb_scatter, ms_zb_sort;
+    float ms_plan;         /* tile pre-pass of the pair kernel (count, scans, plans) */
 } xm_stats;
 
 /* Tuning of the persistent pair kernel (0 = default / autotuned).  A work

@@ -47,7 +47,7 @@ class XmStats(ctypes.Structure):
                 ("ms_build", ctypes.c_float), ("ms_h2d", ctypes.c_float),
                 ("ms_d2h", ctypes.c_float), ("ms_zb_count", ctypes.c_float),
                 ("ms_zb_scan", ctypes.c_float), ("ms_zb_scatter", ctypes.c_float),
-                ("ms_zb_sort", ctypes.c_float)]
+                ("ms_zb_sort", ctypes.c_float), ("ms_plan", ctypes.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -179,6 +179,7 @@ extern "C" xm_status xm_ctx_create(int device, xm_ctx **out)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&ctx->counters, 16 * sizeof(unsigned long long))) != cudaSuccess) return fail(e);
     if ((e = cudaMallocHost(&ctx->h_counters, 16 * sizeof(unsigned long long))) != cudaSuccess) return fail(e);
+    if ((e = cudaMallocHost(&ctx->h_tiles, 2 * sizeof(uint32_t))) != cudaSuccess) return fail(e);
     *out = ctx;
     return XM_OK;
 }
@@ -202,9 +203,11 @@ extern "C" xm_status xm_ctx_destroy(xm_ctx *ctx)
     for (auto &kv : ctx->alpha_cache) xm_dev_free(ctx, kv.second.dev);
     xm_dev_free(ctx, ctx->d_jobs);
     xm_dev_free(ctx, ctx->d_work);
+    xm_dev_free(ctx, ctx->d_plans);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->counters) cudaFree(ctx->counters);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+    if (ctx->h_tiles) cudaFreeHost(ctx->h_tiles);
     for (auto &ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
@@ -356,6 +359,7 @@ extern "C" xm_status xm_segment_free(xm_segment *seg)
     xm_dev_free(ctx, seg->id);
     xm_dev_free(ctx, seg->radec);
     xm_dev_free(ctx, seg->xyz);
+    xm_dev_free(ctx, seg->xyz64);
     xm_dev_free(ctx, seg->tmp);
     delete seg;
     return XM_OK;
@@ -418,7 +422,6 @@ xm_status ensure_result(xm_ctx *ctx, uint64_t cap, bool want_job)
 struct Prepared {
     std::vector<xm::JobDev> jobs;
     uint32_t n_items = 0;
-    uint64_t total_a = 0;
     uint64_t cap_guess = 0;
 };
 
@@ -448,10 +451,12 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
         d.a_id = (const long long *)A->id;
         d.a_radec = A->radec;
         d.a_xyz = A->xyz;
+        d.a_xyz64 = A->xyz64;
         d.a_zoff = A->zone_off;
         d.b_id = (const long long *)B->id;
         d.b_radec = B->radec;
         d.b_xyz = B->xyz;
+        d.b_xyz64 = B->xyz64;
         d.b_zoff = B->zone_off;
         d.alpha = alpha;
         d.sr_rad = p.sr_rad;
@@ -467,7 +472,6 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
         d.item_begin = (uint32_t)items;
         if (A->n > 0 && B->n > 0 && A->z_hi >= A->z_lo) {
             items += ((uint64_t)(A->z_hi - A->z_lo) + zc) / zc;
-            P.total_a += A->n;
         }
         guess += 2 * std::max(A->n, B->n);   // Worker.cu:296-297 default
         if (items >= 0xFFFFFF00ull) {
@@ -513,16 +517,11 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
     }
     XM_CUDA(ctx, cudaMemcpyAsync(ctx->d_jobs, P.jobs.data(), jb, cudaMemcpyHostToDevice, st));
     XM_TRY(ensure_result(ctx, std::max<uint64_t>(ctx->res.cap, P.cap_guess), want_job));
-    // tile pre-pass buffers
-    const uint64_t max_tiles = xm::plan_bound(P.n_items, P.total_a, L.tile);
-    if (max_tiles >= 0xFFFFFF00ull) {
-        ctx->last_error = "too many tiles in one launch";
-        return XM_ERR_INVALID;
-    }
-    const size_t cnt_b = ((size_t)P.n_items * 4 + 255) & ~(size_t)255;
-    const size_t off_b = ((size_t)(P.n_items + 1) * 4 + 255) & ~(size_t)255;
+    // tile pre-pass: count tiles per work item, read the totals back, size the plans
+    const size_t cnt_b = ((size_t)P.n_items * 8 + 255) & ~(size_t)255;
+    const size_t off_b = ((size_t)(P.n_items + 1) * 8 + 255) & ~(size_t)255;
     const size_t scan_b = (xm_scan_tmp_bytes(P.n_items) + 255) & ~(size_t)255;
-    const size_t need = cnt_b + off_b + scan_b + xm::plan_bytes(max_tiles) + 256;
+    const size_t need = cnt_b + off_b + scan_b;
     if (ctx->d_work_bytes < need) {
         xm_dev_free(ctx, ctx->d_work);
         ctx->d_work = nullptr;
@@ -534,9 +533,31 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
     uint32_t *tile_cnt = (uint32_t *)wp;
     uint32_t *tile_off = (uint32_t *)(wp + cnt_b);
     void *scan_tmp = wp + cnt_b + off_b;
-    void *plans = wp + cnt_b + off_b + scan_b;
+    uint32_t n_normal = 0, n_heavy = 0;
+    XM_CUDA(ctx, cudaEventRecord(ctx->ev[14], st));
+    if (P.n_items > 0) {
+        XM_CUDA(ctx, xm::plan_count(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_items, tile_cnt, tile_off,
+                                    scan_tmp, st));
+        XM_CUDA(ctx, cudaMemcpyAsync(ctx->h_tiles, tile_off + P.n_items, 4, cudaMemcpyDeviceToHost, st));
+        XM_CUDA(ctx, cudaMemcpyAsync(ctx->h_tiles + 1, tile_off + 2 * P.n_items + 1, 4, cudaMemcpyDeviceToHost, st));
+        XM_CUDA(ctx, cudaStreamSynchronize(st));
+        n_normal = ctx->h_tiles[0];
+        n_heavy = ctx->h_tiles[1];
+        if ((uint64_t)n_normal + n_heavy >= 0xFFFFFF00ull) {
+            ctx->last_error = "too many tiles in one launch";
+            return XM_ERR_INVALID;
+        }
+        const size_t pb = xm::plan_bytes((uint64_t)n_normal + n_heavy) + 256;
+        if (ctx->d_plans_bytes < pb) {
+            xm_dev_free(ctx, ctx->d_plans);
+            ctx->d_plans = nullptr;
+            ctx->d_plans_bytes = 0;
+            XM_TRY(xm_dev_alloc(ctx, &ctx->d_plans, pb + pb / 4));
+            ctx->d_plans_bytes = pb + pb / 4;
+        }
+    }
     uint32_t retries = 0;
-    float ms = 0;
+    float ms = 0, plan_ms = 0;
     for (;;) {
         XM_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16 * sizeof(unsigned long long), st));
         xm::MatchOut out;
@@ -545,15 +566,18 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         out.job = want_job ? ctx->res.job : nullptr;
         out.cap = ctx->res.cap;
         out.counters = ctx->counters;
+        if (P.n_items > 0 && retries == 0)
+            XM_CUDA(ctx, xm::plan_make(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_items, tile_off, n_normal,
+                                       n_heavy, ctx->d_plans, ctx->counters + 7, st));
         XM_CUDA(ctx, cudaEventRecord(ctx->ev[2], st));
         if (P.n_items > 0)
-            XM_CUDA(ctx, xm::launch_pairs(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_items, plans, tile_cnt,
-                                          tile_off, scan_tmp, (uint32_t)max_tiles, out, st));
+            XM_CUDA(ctx, xm::run_pairs(L, (const xm::JobDev *)ctx->d_jobs, ctx->d_plans, n_normal, n_heavy, out, st));
         XM_CUDA(ctx, cudaEventRecord(ctx->ev[3], st));
         XM_CUDA(ctx, cudaMemcpyAsync(ctx->h_counters, ctx->counters, 16 * sizeof(unsigned long long),
                                      cudaMemcpyDeviceToHost, st));
         XM_CUDA(ctx, cudaStreamSynchronize(st));
         cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        if (retries == 0) cudaEventElapsedTime(&plan_ms, ctx->ev[14], ctx->ev[2]);
         if (ctx->h_counters[7]) {
             ctx->last_error = "pair kernel: a bounded wait for staged data ran out, or the tile plan overflowed";
             return XM_ERR_TIMEOUT;
@@ -579,8 +603,9 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         stats->n_cand += ctx->h_counters[3];
         stats->n_border += ctx->h_counters[4];
         stats->n_exact += ctx->h_counters[5];
-        stats->n_tiles += P.n_items;
-        stats->n_launches += (P.n_items > 0 ? 6 : 0) * (retries + 1);   // count, 3 scan, plans, pairs
+        stats->n_tiles += (uint64_t)n_normal + n_heavy;
+        stats->n_launches += P.n_items > 0 ? 9 + retries : 0;   // count, 2 x 3 scan, plans, pairs
+        stats->ms_plan += plan_ms;
         stats->n_retries += retries;
         stats->ms_match += ms;
     }

@@ -11,6 +11,7 @@
 //   id[n]                  int64
 //   radec[n]               double2 radians, deg / RAD2DEG (Sorter.cu:52-62)
 //   xyz[n]                 float4: FP32 unit vector, w = raq bits
+//   xyz64[3n]              FP64 unit vector (the project sincos, Worker.cu:31-40)
 // zone = floor((dec + 90) / zh) (Sorter.cu:20-24); raq = the leading
 // raq_bits of floor(ra_rad * 2^31 / pi), a monotone quantisation of ra (its
 // step is 2 pi / 2^raq_bits, 2.3e-8 rad for raq_bits = 28), so within a zone
@@ -243,7 +244,8 @@ rs_downsweep(const unsigned long long *__restrict__ keys_in, const uint32_t *__r
 
 __global__ void zb_gather(const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ vals,
                           const xm_obj *__restrict__ objs, unsigned long long n_kept, unsigned long long raq_mask,
-                          long long *__restrict__ id, double2 *__restrict__ radec, float4 *__restrict__ xyz)
+                          long long *__restrict__ id, double2 *__restrict__ radec, float4 *__restrict__ xyz,
+                          double *__restrict__ xyz64)
 {
     for (unsigned long long j = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j < n_kept;
          j += (unsigned long long)gridDim.x * blockDim.x) {
@@ -256,6 +258,11 @@ __global__ void zb_gather(const unsigned long long *__restrict__ keys, const uin
         radec[j] = make_double2(ra, dec);
         xyz[j] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z),
                              __uint_as_float((uint32_t)(keys[j] & raq_mask)));
+        if (xyz64) {
+            xyz64[3 * j] = x;
+            xyz64[3 * j + 1] = y;
+            xyz64[3 * j + 2] = z;
+        }
     }
 }
 
@@ -351,12 +358,14 @@ xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stat
         xm_dev_free(ctx, seg->id);
         xm_dev_free(ctx, seg->radec);
         xm_dev_free(ctx, seg->xyz);
-        seg->id = nullptr; seg->radec = nullptr; seg->xyz = nullptr;
+        xm_dev_free(ctx, seg->xyz64);
+        seg->id = nullptr; seg->radec = nullptr; seg->xyz = nullptr; seg->xyz64 = nullptr;
         seg->cap = 0;
         uint64_t c = std::max<uint64_t>(n, 1);
         XM_TRY(xm_dev_alloc(ctx, (void **)&seg->id, (c + 2) * sizeof(int64_t)));
         XM_TRY(xm_dev_alloc(ctx, (void **)&seg->radec, c * sizeof(double2)));
         XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz, c * sizeof(float4)));
+        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz64, (c + 2) * 3 * sizeof(double)));
         seg->cap = c;
     }
     if (!seg->zone_off) {
@@ -429,7 +438,7 @@ xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stat
         const unsigned long long mask = (1ull << raq_bits) - 1;
         zb_gather<<<grid_for(seg->n, 256, ctx->sm_count, 8), 256, 0, st>>>(kin, vin, objs, seg->n, mask,
                                                                             (long long *)seg->id, seg->radec,
-                                                                            seg->xyz);
+                                                                            seg->xyz, seg->xyz64);
         launches++;
     }
     XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0xFF, ((size_t)nz + 1) * 4, st));
@@ -565,7 +574,7 @@ extern "C" xm_status xm_segment_build_noalloc(int device, void *stream, const xm
     if (kept > 0)
         zb_gather<<<grid_for(kept, 256, sm_count, 8), 256, 0, st>>>(kin, vin, objs, kept, (1ull << raq_bits) - 1,
                                                                     (long long *)out_id, (double2 *)out_radec,
-                                                                    (float4 *)out_xyz);
+                                                                    (float4 *)out_xyz, nullptr);
     if (cudaMemsetAsync(out_zone_off, 0xFF, ((size_t)nz + 1) * 4, st) != cudaSuccess) return XM_ERR_CUDA;
     if (n > 0) zb_bounds_mark<<<grid_for(n, 256, sm_count, 8), 256, 0, st>>>(kin, n, raq_bits, nz, out_zone_off);
     zb_bounds_fill<<<grid_for((uint64_t)nz + 1, 256, sm_count, 8), 256, 0, st>>>(kin, n, raq_bits, nz, out_zone_off);

@@ -46,8 +46,11 @@ struct xm_ctx {
     // job table and tile pre-pass buffers
     void *d_jobs = nullptr;
     size_t d_jobs_bytes = 0;
-    void *d_work = nullptr;      // tile counts, offsets, scan scratch, plans
+    void *d_work = nullptr;      // tile counts, offsets, scan scratch
     size_t d_work_bytes = 0;
+    void *d_plans = nullptr;     // tile plans
+    size_t d_plans_bytes = 0;
+    uint32_t *h_tiles = nullptr; // pinned: tile totals read back after the count pass
 };
 
 struct xm_segment {
@@ -65,7 +68,8 @@ struct xm_segment {
                                    // pads 16-byte bulk copies of zone-offset slices
     int64_t *id = nullptr;
     double2 *radec = nullptr;      // radians
-    float4 *xyz = nullptr;         // FP32 unit vector; w = zone id bits
+    float4 *xyz = nullptr;         // FP32 unit vector; w = quantised-ra bits
+    double *xyz64 = nullptr;       // FP64 unit vector (x, y, z) per object, 2 spare objects
     // scratch kept for rebuilds
     void *tmp = nullptr;           // radix-sort scratch
     size_t tmp_bytes = 0;

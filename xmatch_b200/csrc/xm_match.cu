@@ -168,6 +168,7 @@ struct AObj {
     float fx, fy, fz;
     double alpha;
     long long id;
+    uint32_t gi;        // index in the A segment
     int zone;
     bool full_ring;     // alpha >= 3: every object of a zone is a candidate
     bool have_xyz;
@@ -184,7 +185,7 @@ struct BView {
     const float4 *xyz;
     bool staged, whole;
     int band_lo;
-    uint32_t base;
+    uint32_t base, len;     // WHOLE: staged objects are [base, base + len) of the segment
     const uint32_t *off;
     const uint32_t *g;
     const uint32_t *zoff;
@@ -273,8 +274,8 @@ __device__ __forceinline__ bool next_candidate(const BView &V, const AObj &a, Cu
         if (c.zb > c.zb_end) return false;
         if (V.whole) {
             const int k = c.zb - V.band_lo;
-            c.b0 = V.zoff[k] - V.base;
-            c.b1 = V.zoff[k + 1] - V.base;
+            c.b0 = min(max(V.zoff[k], V.base), V.base + V.len) - V.base;
+            c.b1 = min(max(V.zoff[k + 1], V.base), V.base + V.len) - V.base;
         } else if (V.staged) {
             const int k = c.zb - V.band_lo;
             c.b0 = V.off[k];
@@ -443,8 +444,8 @@ __device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, 
         uint32_t b0, b1;
         const int k = zb - V.band_lo;
         if (V.whole) {
-            b0 = V.zoff[k] - V.base;
-            b1 = V.zoff[k + 1] - V.base;
+            b0 = min(max(V.zoff[k], V.base), V.base + V.len) - V.base;
+            b1 = min(max(V.zoff[k + 1], V.base), V.base + V.len) - V.base;
         } else {
             b0 = V.off[k];
             b1 = V.off[k + 1];
@@ -533,12 +534,14 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
                 cn.exact++;
                 if (cuts_pass(J, a, rb)) {
                     if (!a.have_xyz) {
-                        radec2xyz(a.ra, a.dec, a.x, a.y, a.z);
+                        a.x = __ldg(&J.a_xyz64[3 * (size_t)a.gi]);
+                        a.y = __ldg(&J.a_xyz64[3 * (size_t)a.gi + 1]);
+                        a.z = __ldg(&J.a_xyz64[3 * (size_t)a.gi + 2]);
                         a.have_xyz = true;
                     }
-                    double x2, y2, z2;
-                    radec2xyz(rb.x, rb.y, x2, y2, z2);
-                    c2 = chord2(a.x, a.y, a.z, x2, y2, z2);
+                    const size_t gb = 3 * (size_t)global_index(V, c.zb, q);
+                    c2 = chord2(a.x, a.y, a.z, __ldg(&J.b_xyz64[gb]), __ldg(&J.b_xyz64[gb + 1]),
+                                __ldg(&J.b_xyz64[gb + 2]));
                     m = c2 < J.sr_dist2;
                 }
             }
@@ -568,6 +571,8 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
 // ---------------------------------------------------------------------------
 constexpr int kMaxBand = 72;       // B zones a staged band may span
 constexpr int kMaxPlanSeg = 4;     // per-zone windows of a UNION plan
+constexpr uint32_t kHeavyPairs = 16384;   // pairs above which a full-ring tile is split along B
+constexpr uint32_t kMaxPieces = 1024;
 
 enum : uint32_t { PLAN_WHOLE = 0, PLAN_UNION = 1, PLAN_GLOBAL = 2 };
 
@@ -627,26 +632,63 @@ __device__ __forceinline__ void for_each_tile(const JobDev &J, uint32_t item, ui
     }
 }
 
+// A tile whose zones have no RA cut (alpha >= 3, near the poles) tests its
+// whole B band.  When that is many pairs it is split along B into pieces of
+// at most cap_b objects, each staged and tested as its own plan; pieces go
+// to the "heavy" queue that the pair kernel hands out first, one at a time.
+// Returns the number of pieces (1 = not split) and the piece size.
+__device__ __forceinline__ uint32_t tile_pieces(const JobDev &J, uint32_t len, int zf, int zl, uint32_t cap_b,
+                                                uint32_t *piece)
+{
+    const int band_lo = max(0, zf - J.nz), band_hi = min(J.n_zones - 1, zl + J.nz);
+    const uint32_t nseg = (uint32_t)(band_hi - band_lo + 1);
+    const uint32_t b_len = J.b_zoff[band_hi + 1] - J.b_zoff[band_lo];
+    *piece = b_len;
+    const bool full_ring = J.alpha[zf] >= 3.0 || J.alpha[zl] >= 3.0;
+    if (!full_ring || (int)nseg > kMaxBand || (uint64_t)len * b_len <= kHeavyPairs) return 1;
+    uint32_t pc = max(32u, kHeavyPairs / max(len, 1u));
+    pc = min(pc, cap_b);
+    uint32_t n = (b_len + pc - 1) / pc;
+    if (n > kMaxPieces) {
+        pc = (b_len + kMaxPieces - 1) / kMaxPieces;
+        if (pc > cap_b) return 1;
+        n = (b_len + pc - 1) / pc;   // every piece starts inside the band
+    }
+    if (n <= 1) return 1;
+    *piece = pc;
+    return n;
+}
+
+// Tiles per work item: cnt[item] normal plans, cnt[n_items + item] heavy pieces.
 __global__ void tiles_count(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32_t zc,
-                            uint32_t tile, uint32_t *__restrict__ cnt)
+                            uint32_t tile, uint32_t cap_b, uint32_t *__restrict__ cnt)
 {
     const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
     if (item >= n_items) return;
     const JobDev &J = jobs[n_jobs > 1 ? find_job(jobs, n_jobs, item) : 0];
-    uint32_t c = 0;
-    for_each_tile(J, item, zc, tile, [&](uint32_t, uint32_t, int, int) { ++c; });
+    uint32_t c = 0, h = 0;
+    for_each_tile(J, item, zc, tile, [&](uint32_t, uint32_t len, int zf, int zl) {
+        uint32_t piece;
+        const uint32_t n = tile_pieces(J, len, zf, zl, cap_b, &piece);
+        if (n > 1) h += n; else ++c;
+    });
     cnt[item] = c;
+    cnt[n_items + item] = h;
 }
 
+// Plans: heavy pieces first (off[n_items + item] within [0, n_heavy)), then the
+// normal ones (n_heavy + off[item]).
 __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32_t zc, uint32_t tile,
-                           uint32_t cap_b, const uint32_t *__restrict__ off, TilePlan *__restrict__ plans,
-                           uint32_t max_tiles, unsigned long long *err)
+                           uint32_t cap_b, const uint32_t *__restrict__ off_n, const uint32_t *__restrict__ off_h,
+                           TilePlan *__restrict__ plans, uint32_t max_tiles, unsigned long long *err)
 {
     const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
     if (item >= n_items) return;
     const int jx = n_jobs > 1 ? find_job(jobs, n_jobs, item) : 0;
     const JobDev &J = jobs[jx];
-    uint32_t o = off[item];
+    const uint32_t n_heavy = off_h[n_items];
+    uint32_t o = n_heavy + off_n[item];
+    uint32_t oh = off_h[item];
     for_each_tile(J, item, zc, tile, [&](uint32_t start, uint32_t len, int zf, int zl) {
         TilePlan P;
         P.a_start = start;
@@ -659,8 +701,23 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
         const uint32_t B0 = J.b_zoff[band_lo], B1 = J.b_zoff[band_hi + 1];
         P.b_start = B0;
         P.b_len = B1 - B0;
-        uint32_t mode = PLAN_GLOBAL;
         for (int k = 0; k < kMaxPlanSeg; ++k) P.seg_g[k] = P.seg_len[k] = 0;
+        const uint32_t zword = (min(nseg, 255u) << 8) | ((uint32_t)(zl - zf) << 16);
+        uint32_t piece;
+        const uint32_t npc = tile_pieces(J, len, zf, zl, cap_b, &piece);
+        if (npc > 1) {
+            // heavy: WHOLE plans over consecutive B pieces of the band
+            for (uint32_t q = 0; q < npc; ++q) {
+                P.b_start = B0 + q * piece;
+                P.b_len = min(piece, B1 - P.b_start);
+                P.mode = PLAN_WHOLE | zword;
+                if (oh < max_tiles) plans[oh] = P;
+                else atomicExch(err, 1ull);
+                ++oh;
+            }
+            return;
+        }
+        uint32_t mode = PLAN_GLOBAL;
         if ((int)nseg <= kMaxBand && P.b_len <= cap_b) {
             mode = PLAN_WHOLE;
         } else if (zf == zl && (int)nseg <= kMaxPlanSeg && J.alpha[zf] < 3.0) {
@@ -695,7 +752,7 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
             }
         }
         // nseg is only read for WHOLE (<= kMaxBand) and UNION (<= kMaxPlanSeg) plans
-        P.mode = mode | (min(nseg, 255u) << 8) | ((uint32_t)(zl - zf) << 16);
+        P.mode = mode | zword;
         if (o < max_tiles) plans[o] = P;
         else atomicExch(err, 1ull);
         ++o;
@@ -718,15 +775,15 @@ struct StageT {
     // descriptor (written by the producer before the full-barrier arrive)
     uint32_t a_start, a_len, mode, nseg;
     int32_t band_lo, zf, zl;
-    uint32_t job, b_start, id_skew, zoff_skew, done;
+    uint32_t job, b_start, b_len, id_skew, zoff_skew, done;
     uint32_t seg_off[kMaxPlanSeg + 1];
     uint32_t seg_g[kMaxPlanSeg];
 };
 
 template <int TILE, int VARIANT, bool COUNT_CAND, bool DIST>
 __global__ void __launch_bounds__(TILE + 32, TILE <= 128 ? 4 : 2)
-pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
-            const uint32_t *__restrict__ n_tiles_ptr, uint32_t max_tiles, uint32_t chunk, MatchOut out)
+pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans, uint32_t n_heavy,
+            uint32_t n_normal, uint32_t chunk, MatchOut out)
 {
     using Stage = StageT<TILE>;
     constexpr int C = TILE / 32;   // consumer warps
@@ -739,7 +796,6 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
 
     const int warp = threadIdx.x >> 5;
     const unsigned lane = threadIdx.x & 31;
-    const uint32_t n_tiles = min(*n_tiles_ptr, max_tiles);
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&full[s], 1);
@@ -752,33 +808,127 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
 
     if (warp == 0) {
         // ================= producer =================
-        // Claims `chunk` (<= 32) tiles at a time; lane k prefetches plan k of
-        // the claim, lane 0 issues the copies.  The next claim is requested
-        // before the current one is issued, so its latency overlaps.
+        // Heavy pieces first, one per claim; then normal tiles, `chunk` (<= 32)
+        // per claim, lane k prefetching plan k of the claim; lane 0 issues the
+        // copies.  The next claim is requested before the current one is issued.
         int s = 0;
         uint32_t phase = 0;
         bool ok = true;
         int issued = 0;
-        const uint32_t ch = min(chunk, 32u);
-        uint32_t t0 = 0;
-        if (lane == 0) t0 = (uint32_t)atomicAdd(&out.counters[1], (unsigned long long)ch);
-        t0 = __shfl_sync(0xffffffffu, t0, 0);
         int cached_job = -1;
         const double2 *a_radec = nullptr, *b_radec = nullptr;
         const float4 *a_xyz = nullptr, *b_xyz = nullptr;
         const long long *a_id = nullptr;
         const uint32_t *b_zoff = nullptr;
-        while (ok && t0 < n_tiles) {
-            const uint32_t nt = min(ch, n_tiles - t0);
+        // issue plan words w[16] into the next stage
+        auto issue = [&](const uint32_t (&w)[16]) -> bool {
+            if (!mbar_wait(&empty[s], phase ^ 1u)) return false;
+            if (lane == 0) {
+                const uint32_t a_start = w[0], a_len = w[1], mode = w[2] & 255u, nseg = (w[2] >> 8) & 255u;
+                const int zf = (int)w[3];
+                const int zl = zf + (int)(w[2] >> 16);
+                const int band_lo = (int)w[4];
+                const uint32_t job = w[5], b_start = w[6], b_len = w[7];
+                if ((int)job != cached_job) {
+                    const JobDev &J = jobs[job];
+                    a_radec = J.a_radec; a_xyz = J.a_xyz; a_id = J.a_id;
+                    b_radec = J.b_radec; b_xyz = J.b_xyz; b_zoff = J.b_zoff;
+                    cached_job = (int)job;
+                }
+                Stage &S = stages[s];
+                S.a_start = a_start;
+                S.a_len = a_len;
+                S.mode = mode;
+                S.nseg = nseg;
+                S.band_lo = band_lo;
+                S.zf = zf;
+                S.zl = zl;
+                S.job = job;
+                S.b_start = b_start;
+                S.b_len = b_len;
+                S.done = 0;
+                const uint32_t a_even = a_start & ~1u;
+                S.id_skew = a_start - a_even;
+                const uint32_t id_cnt = (a_start + a_len - a_even + 1) & ~1u;
+                uint32_t bytes = a_len * 32u + id_cnt * 8u;
+                uint32_t zcopy = 0, z_al = 0;
+                if (mode == PLAN_WHOLE) {
+                    bytes += b_len * 32u;
+                    z_al = (uint32_t)band_lo & ~3u;
+                    S.zoff_skew = (uint32_t)band_lo - z_al;
+                    zcopy = (S.zoff_skew + nseg + 1 + 3) & ~3u;
+                    bytes += zcopy * 4u;
+                } else if (mode == PLAN_UNION) {
+                    bytes += b_len * 32u;
+                    uint32_t o = 0;
+#pragma unroll
+                    for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
+                        if (q < nseg) {
+                            S.seg_off[q] = o;
+                            S.seg_g[q] = w[8 + q];
+                            o += w[12 + q];
+                        }
+                    }
+                    S.seg_off[nseg] = o;
+                }
+                fence_proxy_async();
+                mbar_expect_tx(&full[s], bytes);
+                bulk_g2s(S.a_radec, a_radec + a_start, a_len * 16u, &full[s]);
+                bulk_g2s(S.a_xyz, a_xyz + a_start, a_len * 16u, &full[s]);
+                bulk_g2s(S.a_id, a_id + a_even, id_cnt * 8u, &full[s]);
+                if (mode == PLAN_WHOLE) {
+                    if (b_len) {
+                        bulk_g2s(S.b_radec, b_radec + b_start, b_len * 16u, &full[s]);
+                        bulk_g2s(S.b_xyz, b_xyz + b_start, b_len * 16u, &full[s]);
+                    }
+                    bulk_g2s(S.zoff, b_zoff + z_al, zcopy * 4u, &full[s]);
+                } else if (mode == PLAN_UNION) {
+#pragma unroll
+                    for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
+                        const uint32_t ln = w[12 + q];
+                        if (q >= nseg || !ln) continue;
+                        bulk_g2s(S.b_radec + S.seg_off[q], b_radec + w[8 + q], ln * 16u, &full[s]);
+                        bulk_g2s(S.b_xyz + S.seg_off[q], b_xyz + w[8 + q], ln * 16u, &full[s]);
+                    }
+                }
+            }
+            __syncwarp();
+            issued++;
+            if (++s == kStages) {
+                s = 0;
+                phase ^= 1u;
+            }
+            return true;
+        };
+        // ---- heavy queue ----
+        while (ok) {
+            uint32_t h = 0;
+            if (lane == 0) h = (uint32_t)atomicAdd(&out.counters[6], 1ull);
+            h = __shfl_sync(0xffffffffu, h, 0);
+            if (h >= n_heavy) break;
+            uint4 pw[4];
+            const uint4 *src = reinterpret_cast<const uint4 *>(plans + h);
+            pw[0] = src[0]; pw[1] = src[1]; pw[2] = src[2]; pw[3] = src[3];
+            uint32_t w[16] = {pw[0].x, pw[0].y, pw[0].z, pw[0].w, pw[1].x, pw[1].y, pw[1].z, pw[1].w,
+                              pw[2].x, pw[2].y, pw[2].z, pw[2].w, pw[3].x, pw[3].y, pw[3].z, pw[3].w};
+            ok = issue(w);
+        }
+        // ---- normal queue ----
+        const TilePlan *nplans = plans + n_heavy;
+        const uint32_t ch = min(chunk, 32u);
+        uint32_t t0 = 0;
+        if (lane == 0) t0 = (uint32_t)atomicAdd(&out.counters[1], (unsigned long long)ch);
+        t0 = __shfl_sync(0xffffffffu, t0, 0);
+        while (ok && t0 < n_normal) {
+            const uint32_t nt = min(ch, n_normal - t0);
             uint4 pw[4];
             if (lane < nt) {
-                const uint4 *src = reinterpret_cast<const uint4 *>(plans + t0 + lane);
+                const uint4 *src = reinterpret_cast<const uint4 *>(nplans + t0 + lane);
                 pw[0] = src[0]; pw[1] = src[1]; pw[2] = src[2]; pw[3] = src[3];
             }
             uint32_t t_next = 0;
             if (lane == 0) t_next = (uint32_t)atomicAdd(&out.counters[1], (unsigned long long)ch);
-            for (uint32_t k = 0; k < nt; ++k) {
-                // plan k from lane k
+            for (uint32_t k = 0; k < nt && ok; ++k) {
                 uint32_t w[16];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -787,84 +937,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     w[4 * q + 2] = __shfl_sync(0xffffffffu, pw[q].z, k);
                     w[4 * q + 3] = __shfl_sync(0xffffffffu, pw[q].w, k);
                 }
-                if (!mbar_wait(&empty[s], phase ^ 1u)) {
-                    ok = false;
-                    break;
-                }
-                if (lane == 0) {
-                    const uint32_t a_start = w[0], a_len = w[1], mode = w[2] & 255u, nseg = (w[2] >> 8) & 255u;
-                    const int zf = (int)w[3];
-                    const int zl = zf + (int)(w[2] >> 16);
-                    const int band_lo = (int)w[4];
-                    const uint32_t job = w[5], b_start = w[6], b_len = w[7];
-                    if ((int)job != cached_job) {
-                        const JobDev &J = jobs[job];
-                        a_radec = J.a_radec; a_xyz = J.a_xyz; a_id = J.a_id;
-                        b_radec = J.b_radec; b_xyz = J.b_xyz; b_zoff = J.b_zoff;
-                        cached_job = (int)job;
-                    }
-                    Stage &S = stages[s];
-                    S.a_start = a_start;
-                    S.a_len = a_len;
-                    S.mode = mode;
-                    S.nseg = nseg;
-                    S.band_lo = band_lo;
-                    S.zf = zf;
-                    S.zl = zl;
-                    S.job = job;
-                    S.b_start = b_start;
-                    S.done = 0;
-                    const uint32_t a_even = a_start & ~1u;
-                    S.id_skew = a_start - a_even;
-                    const uint32_t id_cnt = (a_start + a_len - a_even + 1) & ~1u;
-                    uint32_t bytes = a_len * 32u + id_cnt * 8u;
-                    uint32_t zcopy = 0, z_al = 0;
-                    if (mode == PLAN_WHOLE) {
-                        bytes += b_len * 32u;
-                        z_al = (uint32_t)band_lo & ~3u;
-                        S.zoff_skew = (uint32_t)band_lo - z_al;
-                        zcopy = (S.zoff_skew + nseg + 1 + 3) & ~3u;
-                        bytes += zcopy * 4u;
-                    } else if (mode == PLAN_UNION) {
-                        bytes += b_len * 32u;
-                        uint32_t o = 0;
-#pragma unroll
-                        for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
-                            if (q < nseg) {
-                                S.seg_off[q] = o;
-                                S.seg_g[q] = w[8 + q];
-                                o += w[12 + q];
-                            }
-                        }
-                        S.seg_off[nseg] = o;
-                    }
-                    fence_proxy_async();
-                    mbar_expect_tx(&full[s], bytes);
-                    bulk_g2s(S.a_radec, a_radec + a_start, a_len * 16u, &full[s]);
-                    bulk_g2s(S.a_xyz, a_xyz + a_start, a_len * 16u, &full[s]);
-                    bulk_g2s(S.a_id, a_id + a_even, id_cnt * 8u, &full[s]);
-                    if (mode == PLAN_WHOLE) {
-                        if (b_len) {
-                            bulk_g2s(S.b_radec, b_radec + b_start, b_len * 16u, &full[s]);
-                            bulk_g2s(S.b_xyz, b_xyz + b_start, b_len * 16u, &full[s]);
-                        }
-                        bulk_g2s(S.zoff, b_zoff + z_al, zcopy * 4u, &full[s]);
-                    } else if (mode == PLAN_UNION) {
-#pragma unroll
-                        for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
-                            const uint32_t ln = w[12 + q];
-                            if (q >= nseg || !ln) continue;
-                            bulk_g2s(S.b_radec + S.seg_off[q], b_radec + w[8 + q], ln * 16u, &full[s]);
-                            bulk_g2s(S.b_xyz + S.seg_off[q], b_xyz + w[8 + q], ln * 16u, &full[s]);
-                        }
-                    }
-                }
-                __syncwarp();
-                issued++;
-                if (++s == kStages) {
-                    s = 0;
-                    phase ^= 1u;
-                }
+                ok = issue(w);
             }
             t0 = __shfl_sync(0xffffffffu, t_next, 0);
         }
@@ -923,6 +996,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 }
                 a.full_ring = a.alpha >= 3.0;
                 a.id = S.a_id[S.id_skew + t];
+                a.gi = S.a_start + t;
                 a.have_xyz = false;
                 BView V;
                 V.staged = false;
@@ -942,6 +1016,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             V.xyz = S.b_xyz;
             V.zoff = S.zoff + S.zoff_skew;
             V.base = S.b_start;
+            V.len = S.b_len;
             V.off = S.seg_off;
             V.g = S.seg_g;
             // ---- phase 1: each lane's candidate ranges ----
@@ -977,6 +1052,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     a.alpha = alpha;
                     a.full_ring = alpha >= 3.0;
                     a.id = S.a_id[S.id_skew + t];
+                    a.gi = S.a_start + t;
+                a.gi = S.a_start + t;
                     a.have_xyz = false;
                     test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
                 }
@@ -1029,10 +1106,11 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                                 cn.border += (c32 >= K.thr_lo) ? 1ull : 0ull;
                                 cn.exact++;
                                 if (cuts_k(K, ra.x, ra.y, al, rb)) {
-                                    double x1, y1, z1, x2, y2, z2;
-                                    radec2xyz(ra.x, ra.y, x1, y1, z1);
-                                    radec2xyz(rb.x, rb.y, x2, y2, z2);
-                                    c2 = chord2(x1, y1, z1, x2, y2, z2);
+                                    const size_t ga = 3 * (size_t)(S.a_start + ta);
+                                    const size_t gb = 3 * (size_t)staged_global(V, (int)S.nseg, q);
+                                    c2 = chord2(__ldg(&J.a_xyz64[ga]), __ldg(&J.a_xyz64[ga + 1]), __ldg(&J.a_xyz64[ga + 2]),
+                                                __ldg(&J.b_xyz64[gb]), __ldg(&J.b_xyz64[gb + 1]),
+                                                __ldg(&J.b_xyz64[gb + 2]));
                                     m = c2 < K.sr_dist2;
                                 }
                             }
@@ -1091,8 +1169,8 @@ constexpr size_t smem_bytes()
 }
 
 template <int TILE, int VARIANT, bool CC, bool DIST>
-cudaError_t launch_t(const LaunchCfg &L, const JobDev *jobs, const TilePlan *plans, const uint32_t *n_tiles,
-                     uint32_t max_tiles, const MatchOut &out, cudaStream_t st)
+cudaError_t launch_t(const LaunchCfg &L, const JobDev *jobs, const TilePlan *plans, uint32_t n_heavy,
+                     uint32_t n_normal, const MatchOut &out, cudaStream_t st)
 {
     auto k = pair_kernel<TILE, VARIANT, CC, DIST>;
     const size_t smem = smem_bytes<TILE>();
@@ -1107,55 +1185,57 @@ cudaError_t launch_t(const LaunchCfg &L, const JobDev *jobs, const TilePlan *pla
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, TILE + 32, smem);
         if (per_sm < 1) per_sm = 1;
     }
-    const uint64_t want = ((uint64_t)max_tiles + L.chunk - 1) / L.chunk;
+    const uint64_t want = (uint64_t)n_heavy + ((uint64_t)n_normal + L.chunk - 1) / L.chunk;
     unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)L.sm_count * per_sm, std::max<uint64_t>(want, 1));
-    k<<<grid, TILE + 32, smem, st>>>(jobs, plans, n_tiles, max_tiles, L.chunk, out);
+    k<<<grid, TILE + 32, smem, st>>>(jobs, plans, n_heavy, n_normal, L.chunk, out);
     return cudaGetLastError();
 }
 
 template <int TILE>
-cudaError_t launch_tile(const LaunchCfg &L, const JobDev *jobs, const TilePlan *plans, const uint32_t *n_tiles,
-                        uint32_t max_tiles, const MatchOut &out, cudaStream_t st)
+cudaError_t launch_tile(const LaunchCfg &L, const JobDev *jobs, const TilePlan *plans, uint32_t n_heavy,
+                        uint32_t n_normal, const MatchOut &out, cudaStream_t st)
 {
     if (L.variant == 1)
-        return L.dist ? launch_t<TILE, 1, true, true>(L, jobs, plans, n_tiles, max_tiles, out, st)
-                      : launch_t<TILE, 1, true, false>(L, jobs, plans, n_tiles, max_tiles, out, st);
+        return L.dist ? launch_t<TILE, 1, true, true>(L, jobs, plans, n_heavy, n_normal, out, st)
+                      : launch_t<TILE, 1, true, false>(L, jobs, plans, n_heavy, n_normal, out, st);
     if (L.count_cand)
-        return L.dist ? launch_t<TILE, 0, true, true>(L, jobs, plans, n_tiles, max_tiles, out, st)
-                      : launch_t<TILE, 0, true, false>(L, jobs, plans, n_tiles, max_tiles, out, st);
-    return L.dist ? launch_t<TILE, 0, false, true>(L, jobs, plans, n_tiles, max_tiles, out, st)
-                  : launch_t<TILE, 0, false, false>(L, jobs, plans, n_tiles, max_tiles, out, st);
+        return L.dist ? launch_t<TILE, 0, true, true>(L, jobs, plans, n_heavy, n_normal, out, st)
+                      : launch_t<TILE, 0, true, false>(L, jobs, plans, n_heavy, n_normal, out, st);
+    return L.dist ? launch_t<TILE, 0, false, true>(L, jobs, plans, n_heavy, n_normal, out, st)
+                  : launch_t<TILE, 0, false, false>(L, jobs, plans, n_heavy, n_normal, out, st);
 }
 
 }  // namespace
 
-uint64_t plan_bound(uint32_t n_items, uint64_t total_a, int tile)
-{
-    // a tile holds more than tile/2 objects unless it ends a work item or
-    // precedes a large zone (which then holds more than tile/2)
-    return (uint64_t)n_items + 2 * (4 * total_a / (uint64_t)tile + 1) + 1;
-}
-
 size_t plan_bytes(uint64_t n_plans) { return (size_t)n_plans * sizeof(TilePlan); }
 
-cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, void *plans,
-                         uint32_t *tile_cnt, uint32_t *tile_off, void *scan_tmp, uint32_t max_tiles,
-                         const MatchOut &out, cudaStream_t st)
+cudaError_t plan_count(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, uint32_t *cnt,
+                       uint32_t *off, void *scan_tmp, cudaStream_t st)
 {
     const unsigned g = (n_items + 127) / 128;
-    tiles_count<<<g, 128, 0, st>>>(jobs, n_jobs, n_items, L.zc, (uint32_t)L.tile, tile_cnt);
-    cudaError_t e = xm_scan_exclusive_u32(tile_cnt, tile_off, n_items, scan_tmp, st);
+    tiles_count<<<g, 128, 0, st>>>(jobs, n_jobs, n_items, L.zc, (uint32_t)L.tile, 4u * (uint32_t)L.tile, cnt);
+    cudaError_t e = xm_scan_exclusive_u32(cnt, off, n_items, scan_tmp, st);
     if (e != cudaSuccess) return e;
-    const uint32_t cap_b = 4u * (uint32_t)L.tile;
-    tiles_make<<<g, 128, 0, st>>>(jobs, n_jobs, n_items, L.zc, (uint32_t)L.tile, cap_b, tile_off,
-                                  (TilePlan *)plans, max_tiles, out.counters + 7);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    const uint32_t *n_tiles = tile_off + n_items;
+    return xm_scan_exclusive_u32(cnt + n_items, off + n_items + 1, n_items, scan_tmp, st);
+}
+
+cudaError_t plan_make(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, const uint32_t *off,
+                      uint32_t n_normal, uint32_t n_heavy, void *plans, unsigned long long *err, cudaStream_t st)
+{
+    const unsigned g = (n_items + 127) / 128;
+    tiles_make<<<g, 128, 0, st>>>(jobs, n_jobs, n_items, L.zc, (uint32_t)L.tile, 4u * (uint32_t)L.tile, off,
+                                  off + n_items + 1, (TilePlan *)plans, n_normal + n_heavy, err);
+    return cudaGetLastError();
+}
+
+cudaError_t run_pairs(const LaunchCfg &L, const JobDev *jobs, const void *plans, uint32_t n_normal, uint32_t n_heavy,
+                      const MatchOut &out, cudaStream_t st)
+{
+    const TilePlan *p = (const TilePlan *)plans;
     switch (L.tile) {
-    case 64: return launch_tile<64>(L, jobs, (const TilePlan *)plans, n_tiles, max_tiles, out, st);
-    case 256: return launch_tile<256>(L, jobs, (const TilePlan *)plans, n_tiles, max_tiles, out, st);
-    default: return launch_tile<128>(L, jobs, (const TilePlan *)plans, n_tiles, max_tiles, out, st);
+    case 64: return launch_tile<64>(L, jobs, p, n_heavy, n_normal, out, st);
+    case 256: return launch_tile<256>(L, jobs, p, n_heavy, n_normal, out, st);
+    default: return launch_tile<128>(L, jobs, p, n_heavy, n_normal, out, st);
     }
 }
 

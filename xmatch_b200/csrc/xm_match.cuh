@@ -11,9 +11,11 @@ struct JobDev {
     const double2 *a_radec;
     const float4 *a_xyz;
     const uint32_t *a_zoff;    // [n_zones + 1]
+    const double *a_xyz64;     // [3 nA] FP64 unit vectors
     const long long *b_id;
     const double2 *b_radec;
     const float4 *b_xyz;
+    const double *b_xyz64;
     const uint32_t *b_zoff;    // [n_zones + 1]
     const double *alpha;       // [n_zones] RA half-width of A's zones
     double sr_rad, sr_dist2;
@@ -31,8 +33,8 @@ struct MatchOut {
     double *dist;              // [cap] or null
     uint32_t *job;             // [cap] or null
     unsigned long long cap;
-    // [0] matches, [1] next work item, [2] tested, [3] candidates, [4] in margin band,
-    // [5] FP64 decisions, [7] error flag (a bounded wait ran out)
+    // [0] matches, [1] next normal tile, [2] tested, [3] candidates, [4] in margin band,
+    // [5] FP64 decisions, [6] next heavy piece, [7] error flag (a bounded wait ran out)
     unsigned long long *counters;
 };
 
@@ -47,16 +49,19 @@ struct LaunchCfg {
     bool dist = true;
 };
 
-// Upper bound of the number of tiles (plans) for n_items work items over
-// total_a A objects, and the bytes of that many plans.
-uint64_t plan_bound(uint32_t n_items, uint64_t total_a, int tile);
 size_t plan_bytes(uint64_t n_plans);
 
-// Tile pre-pass (count, scan, plans) and the pair kernel, all on `st`.
-// tile_cnt: [n_items], tile_off: [n_items + 1], scan_tmp: xm_scan_tmp_bytes(n_items),
-// plans: plan_bytes(max_tiles) with max_tiles >= plan_bound(...).
-cudaError_t launch_pairs(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, void *plans,
-                         uint32_t *tile_cnt, uint32_t *tile_off, void *scan_tmp, uint32_t max_tiles,
-                         const MatchOut &out, cudaStream_t st);
+// Tile pre-pass, part 1: tiles per work item.  cnt: [2 n_items] (normal, heavy),
+// off: [2 (n_items + 1)] exclusive scans of both halves (totals at off[n_items]
+// and off[2 n_items + 1]), scan_tmp: xm_scan_tmp_bytes(n_items).
+cudaError_t plan_count(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, uint32_t *cnt,
+                       uint32_t *off, void *scan_tmp, cudaStream_t st);
+// Part 2: plans for n_heavy heavy pieces (first) and n_normal tiles; an
+// overflow sets *err.
+cudaError_t plan_make(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, const uint32_t *off,
+                      uint32_t n_normal, uint32_t n_heavy, void *plans, unsigned long long *err, cudaStream_t st);
+// The pair kernel over the plans (counters[6] and counters[1] must be zero).
+cudaError_t run_pairs(const LaunchCfg &L, const JobDev *jobs, const void *plans, uint32_t n_normal, uint32_t n_heavy,
+                      const MatchOut &out, cudaStream_t st);
 
 }  // namespace xm
