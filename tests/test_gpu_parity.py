@@ -139,6 +139,38 @@ def test_oversize_zones(ctx):
     seg.free()
 
 
+def _zone_mix(rng):
+    # zones of 1 .. 300 objects (warp path), one of 5000 (block path), and input
+    # in dec order so that neighbouring records share a zone
+    zh = 2 * ARCSEC
+    sizes = np.concatenate([np.arange(1, 301), [5000]])
+    zone = np.repeat(np.arange(len(sizes)) * 3 + 20_000, sizes)
+    dec = -90 + (zone + rng.uniform(0.1, 0.9, len(zone))) * zh
+    ra = rng.uniform(0, 360, len(zone))
+    ra[: len(ra) // 7] = 180.0            # ties in ra inside a zone
+    return objs(np.arange(len(zone)), ra, dec), zh
+
+
+@pytest.mark.parametrize("case", ["mix_sorted", "mix_shuffled", "one_zone_8192", "one_zone_8193"])
+def test_build_paths_match_oracle_export(ctx, case):
+    rng = np.random.default_rng(21)
+    if case.startswith("mix"):
+        A, zh = _zone_mix(rng)
+        if case == "mix_shuffled":
+            A = A[rng.permutation(len(A))]
+    else:
+        n = int(case.rsplit("_", 1)[1])   # 8192 = largest zone of the block sort
+        zh = 10 * ARCSEC
+        A = objs(np.arange(n), rng.uniform(0, 360, n), rng.uniform(0, 0.0027, n))
+    seg = ctx.build(A, zh)
+    ids, radec, zb, ze = seg.export()
+    oid, ordec, ozb, oze = oracle.build_export(A, zh)
+    assert np.array_equal(ids, oid) and radec.tobytes() == ordec.tobytes()
+    assert np.array_equal(zb, ozb) and np.array_equal(ze, oze)
+    seg.free()
+    check_parity(ctx, A, A, zh / ARCSEC, variants=(0,))
+
+
 def test_empty_single_and_dropped(ctx):
     E = np.empty(0, OBJ_DTYPE)
     one = objs([7], [10.0], [10.0])

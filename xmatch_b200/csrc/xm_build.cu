@@ -295,6 +295,280 @@ __global__ void zb_bounds_fill(const unsigned long long *__restrict__ keys, unsi
     }
 }
 
+// ---------------------------------------------------------------------------
+// Zone-bucket build: objects counted per zone, the counts scanned into the
+// zone offsets, 32-byte records scattered into their zone's bucket through
+// per-zone atomic cursors, then every zone sorted in place by (raq, input
+// index) -- a warp per zone of up to kWarpZone objects (rank by counting), a
+// block per larger zone (bitonic sort in shared memory) up to kBlockZone.
+// ---------------------------------------------------------------------------
+constexpr int kWarpZone = 256;
+constexpr int kBlockZone = 8192;
+constexpr int kZsThreads = 512;
+
+struct ZRec {          // 32 bytes, one per kept object, in its zone's bucket
+    double ra, dec;    // radians
+    long long id;
+    uint32_t raq;      // leading raq_bits of raq32(ra)
+    uint32_t idx;      // input index
+};
+
+// Lanes whose value equals the previous lane's form runs (consecutive equal
+// zones, as in dec-ordered input); the run's first lane acts for the run.
+struct Run {
+    unsigned head;     // first lane of the calling lane's run
+    unsigned len;      // run length (valid on the head lane)
+    bool is_head;
+};
+
+__device__ __forceinline__ Run warp_run(int v, unsigned lane)
+{
+    const int prev = __shfl_up_sync(0xffffffffu, v, 1);
+    const bool h = lane == 0 || prev != v;
+    const unsigned heads = __ballot_sync(0xffffffffu, h);
+    const unsigned le = (2u << lane) - 1u;   // lanes <= lane (all lanes for lane 31)
+    Run r;
+    r.head = 31u - __clz(heads & le);
+    const unsigned after = heads & ~le;
+    r.len = (after ? (unsigned)(__ffs(after) - 1) : 32u) - lane;
+    r.is_head = h;
+    return r;
+}
+
+// Pass 1: objects per zone; populated zone range and dropped count in misc.
+__global__ void zc_count(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp,
+                         uint32_t *__restrict__ cnt, uint32_t *__restrict__ misc)
+{
+    __shared__ unsigned s_lo, s_hi, s_bad;
+    if (threadIdx.x == 0) {
+        s_lo = 0xFFFFFFFFu;
+        s_hi = 0u;
+        s_bad = 0u;
+    }
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31;
+    unsigned zlo = 0xFFFFFFFFu, zhi = 0u, bad = 0u;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long warp0 = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull;
+    for (unsigned long long wb = warp0; wb < n; wb += stride) {
+        const unsigned long long i = wb + lane;
+        int z = -2;
+        if (i < n) {
+            const xm_obj o = objs[i];
+            z = isfinite(o.ra_deg) ? xm::zone_of(o.dec_deg, kp.zh_deg, kp.n_zones) : -1;
+            if (z < 0) {
+                ++bad;
+            } else {
+                zlo = min(zlo, (unsigned)z);
+                zhi = max(zhi, (unsigned)z);
+            }
+        }
+        const Run r = warp_run(z, lane);
+        if (r.is_head && z >= 0) atomicAdd(&cnt[z], r.len);
+    }
+    zlo = __reduce_min_sync(0xffffffffu, zlo);
+    zhi = __reduce_max_sync(0xffffffffu, zhi);
+    bad = __reduce_add_sync(0xffffffffu, bad);
+    if (lane == 0) {
+        atomicMin(&s_lo, zlo);
+        atomicMax(&s_hi, zhi);
+        atomicAdd(&s_bad, bad);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_lo != 0xFFFFFFFFu) atomicMin(&misc[0], s_lo);
+        atomicMax(&misc[1], s_hi);
+        if (s_bad) atomicAdd(&misc[2], s_bad);
+    }
+}
+
+// After the scan: cursor[z] = zone_off[z] (in place of the count), zones above
+// kWarpZone listed for the block sort, largest zone in misc[4], dropped count
+// stored beside the offsets (zone_off[n_zones + 1]).
+__global__ void zc_classify(uint32_t *__restrict__ cnt, uint32_t *__restrict__ zone_off, int n_zones,
+                            uint32_t *__restrict__ big, uint32_t *__restrict__ misc)
+{
+    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z <= n_zones; z += gridDim.x * blockDim.x) {
+        if (z == n_zones) {
+            zone_off[n_zones + 1] = misc[2];
+            continue;
+        }
+        const uint32_t m = cnt[z];
+        cnt[z] = zone_off[z];
+        if (m > (uint32_t)kWarpZone) {
+            big[atomicAdd(&misc[3], 1u)] = (uint32_t)z;
+            atomicMax(&misc[4], m);
+        }
+    }
+}
+
+// Pass 2: every kept object's record into its zone bucket.
+__global__ void zc_scatter(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp,
+                           uint32_t *__restrict__ cursor, ZRec *__restrict__ recs)
+{
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long warp0 = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull;
+    for (unsigned long long wb = warp0; wb < n; wb += stride) {
+        const unsigned long long i = wb + lane;
+        int z = -2;
+        xm_obj o;
+        if (i < n) {
+            o = objs[i];
+            z = isfinite(o.ra_deg) ? xm::zone_of(o.dec_deg, kp.zh_deg, kp.n_zones) : -1;
+        }
+        const Run r = warp_run(z, lane);
+        uint32_t base = 0;
+        if (r.is_head && z >= 0) base = atomicAdd(&cursor[z], r.len);
+        base = __shfl_sync(0xffffffffu, base, r.head);
+        if (z >= 0) {
+            const double ra = __ddiv_rn(o.ra_deg, XM_RAD2DEG);
+            const double dec = __ddiv_rn(o.dec_deg, XM_RAD2DEG);
+            ZRec *q = recs + base + (lane - r.head);
+            reinterpret_cast<double2 *>(q)[0] = make_double2(ra, dec);
+            reinterpret_cast<uint4 *>(q)[1] =
+                make_uint4((uint32_t)(unsigned long long)o.id, (uint32_t)((unsigned long long)o.id >> 32),
+                           xm::raq32(ra) >> kp.raq_shift, (uint32_t)i);
+        }
+    }
+}
+
+struct ZOut {
+    long long *id;
+    double2 *radec;
+    float4 *xyz;
+    double *xyz64;
+};
+
+__device__ __forceinline__ void zs_emit(const ZRec &r, unsigned long long j, const ZOut &o)
+{
+    double x, y, z;
+    xm::radec2xyz(r.ra, r.dec, x, y, z);
+    o.id[j] = r.id;
+    o.radec[j] = make_double2(r.ra, r.dec);
+    o.xyz[j] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z), __uint_as_float(r.raq));
+    o.xyz64[3 * j] = x;
+    o.xyz64[3 * j + 1] = y;
+    o.xyz64[3 * j + 2] = z;
+}
+
+__device__ __forceinline__ ZRec zs_load(const ZRec *p)
+{
+    const double2 a = reinterpret_cast<const double2 *>(p)[0];
+    const uint4 b = reinterpret_cast<const uint4 *>(p)[1];
+    ZRec r;
+    r.ra = a.x;
+    r.dec = a.y;
+    r.id = (long long)(((unsigned long long)b.y << 32) | b.x);
+    r.raq = b.z;
+    r.idx = b.w;
+    return r;
+}
+
+template <int E>
+__device__ __forceinline__ void zs_warp_zone(const ZRec *__restrict__ recs, uint32_t b, uint32_t m,
+                                             unsigned long long *sk, unsigned lane, const ZOut &o)
+{
+    unsigned long long key[E];
+    uint32_t rank[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t k = lane + 32u * e;
+        key[e] = ~0ull;
+        rank[e] = 0;
+        if (k < m) {
+            const uint4 t = reinterpret_cast<const uint4 *>(recs + b + k)[1];
+            key[e] = ((unsigned long long)t.z << 32) | t.w;
+            sk[k] = key[e];
+        }
+    }
+    __syncwarp();
+    for (uint32_t j = 0; j < m; ++j) {
+        const unsigned long long kj = sk[j];
+#pragma unroll
+        for (int e = 0; e < E; ++e) rank[e] += kj < key[e] ? 1u : 0u;
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t k = lane + 32u * e;
+        if (k < m) zs_emit(zs_load(recs + b + k), (unsigned long long)b + rank[e], o);
+    }
+    __syncwarp();
+}
+
+// Zones of at most kWarpZone objects: one warp each, ranks by counting
+// (keys are unique: the input index is part of the key).
+__global__ void __launch_bounds__(256)
+zs_warp(const ZRec *__restrict__ recs, const uint32_t *__restrict__ zone_off, int n_zones, ZOut o)
+{
+    __shared__ unsigned long long skeys[8][kWarpZone];
+    const unsigned lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    unsigned long long *sk = skeys[w];
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int z = gw; z < n_zones; z += nw) {
+        const uint32_t b = zone_off[z];
+        const uint32_t m = zone_off[z + 1] - b;
+        if (m == 0 || m > (uint32_t)kWarpZone) continue;
+        if (m <= 32) zs_warp_zone<1>(recs, b, m, sk, lane, o);
+        else if (m <= 64) zs_warp_zone<2>(recs, b, m, sk, lane, o);
+        else if (m <= 128) zs_warp_zone<4>(recs, b, m, sk, lane, o);
+        else zs_warp_zone<8>(recs, b, m, sk, lane, o);
+    }
+}
+
+// Zones of kWarpZone+1 .. kBlockZone objects: one block each, bitonic sort of
+// (raq, idx) keys padded to a power of two, then records emitted in order.
+__global__ void __launch_bounds__(kZsThreads)
+zs_block(const ZRec *__restrict__ recs, const uint32_t *__restrict__ zone_off, const uint32_t *__restrict__ big,
+         const uint32_t *__restrict__ misc, ZOut o)
+{
+    extern __shared__ __align__(16) unsigned char zs_smem[];
+    unsigned long long *sk = (unsigned long long *)zs_smem;        // [kBlockZone]
+    uint16_t *sp = (uint16_t *)(sk + kBlockZone);                   // [kBlockZone]
+    const uint32_t n_big = misc[3];
+    for (uint32_t q = blockIdx.x; q < n_big; q += gridDim.x) {
+        const uint32_t z = big[q];
+        const uint32_t b = zone_off[z];
+        const uint32_t m = zone_off[z + 1] - b;
+        if (m > (uint32_t)kBlockZone) continue;   // left to the radix-sort build
+        uint32_t P = 1;
+        while (P < m) P <<= 1;
+        for (uint32_t k = threadIdx.x; k < P; k += blockDim.x) {
+            unsigned long long key = ~0ull;
+            if (k < m) {
+                const uint4 t = reinterpret_cast<const uint4 *>(recs + b + k)[1];
+                key = ((unsigned long long)t.z << 32) | t.w;
+            }
+            sk[k] = key;
+            sp[k] = (uint16_t)k;
+        }
+        for (uint32_t size = 2; size <= P; size <<= 1) {
+            for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+                __syncthreads();
+                for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                    const uint32_t i = 2 * t - (t & (stride - 1));
+                    const uint32_t j = i + stride;
+                    const bool up = (i & size) == 0;
+                    const unsigned long long ki = sk[i], kj = sk[j];
+                    if ((ki > kj) == up) {
+                        sk[i] = kj;
+                        sk[j] = ki;
+                        const uint16_t pi = sp[i];
+                        sp[i] = sp[j];
+                        sp[j] = pi;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x)
+            zs_emit(zs_load(recs + b + sp[k]), (unsigned long long)b + k, o);
+        __syncthreads();
+    }
+}
+
 int grid_for(unsigned long long n, int threads, int sm_count, int per_sm = 8)
 {
     unsigned long long blocks = (n + threads - 1) / threads;
@@ -336,7 +610,7 @@ static xm_status ensure(xm_ctx *ctx, void **p, size_t *have, size_t need)
     return XM_OK;
 }
 
-xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stats *stats)
+static xm_status build_lsd(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stats *stats)
 {
     xm_ctx *ctx = seg->ctx;
     cudaStream_t st = ctx->stream;
@@ -469,6 +743,134 @@ xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stat
         stats->n_launches += launches;
     }
     return XM_OK;
+}
+
+static xm_status seg_storage(xm_segment *seg, uint64_t n)
+{
+    xm_ctx *ctx = seg->ctx;
+    if (seg->cap < n || !seg->id) {
+        xm_dev_free(ctx, seg->id);
+        xm_dev_free(ctx, seg->radec);
+        xm_dev_free(ctx, seg->xyz);
+        xm_dev_free(ctx, seg->xyz64);
+        seg->id = nullptr; seg->radec = nullptr; seg->xyz = nullptr; seg->xyz64 = nullptr;
+        seg->cap = 0;
+        uint64_t c = std::max<uint64_t>(n, 1);
+        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->id, (c + 2) * sizeof(int64_t)));
+        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->radec, c * sizeof(double2)));
+        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz, c * sizeof(float4)));
+        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz64, (c + 2) * 3 * sizeof(double)));
+        seg->cap = c;
+    }
+    if (!seg->zone_off) {
+        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->zone_off, ((size_t)seg->n_zones + 8) * 4));
+        XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0, ((size_t)seg->n_zones + 8) * 4, ctx->stream));
+    }
+    return XM_OK;
+}
+
+// Zone-bucket build; *fallback is set when a zone holds more than kBlockZone
+// objects (the radix-sort build then redoes the segment).
+static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stats *stats, bool *fallback)
+{
+    xm_ctx *ctx = seg->ctx;
+    cudaStream_t st = ctx->stream;
+    *fallback = false;
+    const int nz = seg->n_zones;
+    int raq_bits, passes;
+    xm_raq_layout(nz, &raq_bits, &passes);
+    seg->raq_bits = raq_bits;
+    XM_TRY(seg_storage(seg, n));
+    const uint64_t nn = std::max<uint64_t>(n, 1);
+    // scratch: records, per-zone counts/cursors, big-zone list, scan scratch, misc
+    const size_t rb = (nn * sizeof(ZRec) + 255) & ~(size_t)255;
+    const size_t zb = (((size_t)nz + 1) * 4 + 255) & ~(size_t)255;
+    const size_t sb = (xm_scan_tmp_bytes((size_t)nz) + 255) & ~(size_t)255;
+    const size_t mb = 256;
+    XM_TRY(ensure(ctx, &seg->tmp, &seg->tmp_bytes, rb + 2 * zb + sb + mb));
+    char *w = (char *)seg->tmp;
+    ZRec *recs = (ZRec *)w; w += rb;
+    uint32_t *cnt = (uint32_t *)w; w += zb;
+    uint32_t *big = (uint32_t *)w; w += zb;
+    void *scan_tmp = w; w += sb;
+    uint32_t *misc = (uint32_t *)w;   // z_lo, z_hi, dropped, n_big, largest zone
+    uint32_t launches = 0;
+
+    if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[0], st));
+    XM_CUDA(ctx, cudaMemsetAsync(cnt, 0, (size_t)nz * 4, st));
+    XM_CUDA(ctx, cudaMemsetAsync(misc, 0, 32, st));
+    XM_CUDA(ctx, cudaMemsetAsync(misc, 0xFF, 4, st));
+    KeyParams kp{seg->zh_deg, nz, 32 - raq_bits, raq_bits, passes};
+    if (n > 0) {
+        zc_count<<<grid_for(n, 256, ctx->sm_count, 8), 256, 0, st>>>(objs, n, kp, cnt, misc);
+        launches++;
+    }
+    if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[8], st));
+    XM_CUDA(ctx, xm_scan_exclusive_u32(cnt, seg->zone_off, (size_t)nz, scan_tmp, st));
+    zc_classify<<<grid_for((uint64_t)nz + 1, 256, ctx->sm_count, 8), 256, 0, st>>>(cnt, seg->zone_off, nz, big, misc);
+    launches += 4;
+    if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[9], st));
+    if (n > 0) {
+        zc_scatter<<<grid_for(n, 256, ctx->sm_count, 8), 256, 0, st>>>(objs, n, kp, cnt, recs);
+        launches++;
+    }
+    if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[10], st));
+    ZOut o{(long long *)seg->id, seg->radec, seg->xyz, seg->xyz64};
+    if (n > 0) {
+        zs_warp<<<grid_for((uint64_t)nz * 32, 256, ctx->sm_count, 8), 256, 0, st>>>(recs, seg->zone_off, nz, o);
+        static bool attr = false;
+        const size_t smem = (size_t)kBlockZone * 10;
+        if (!attr) {
+            XM_CUDA(ctx, cudaFuncSetAttribute(zs_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr = true;
+        }
+        zs_block<<<ctx->sm_count * 2, kZsThreads, smem, st>>>(recs, seg->zone_off, big, misc, o);
+        launches += 2;
+    }
+    XM_CUDA(ctx, cudaGetLastError());
+    if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[11], st));
+    uint32_t hm[8];
+    XM_CUDA(ctx, cudaMemcpyAsync(hm, misc, 32, cudaMemcpyDeviceToHost, st));
+    XM_CUDA(ctx, cudaStreamSynchronize(st));
+    const uint64_t dropped = n ? hm[2] : 0;
+    seg->n = n - dropped;
+    seg->n_in = n;
+    seg->dropped_host = (uint32_t)dropped;
+    if (seg->n > 0) {
+        seg->z_lo = (int32_t)hm[0];
+        seg->z_hi = (int32_t)hm[1];
+    } else {
+        seg->z_lo = 0;
+        seg->z_hi = -1;
+    }
+    if (hm[4] > (uint32_t)kBlockZone) *fallback = true;
+    if (stats) {
+        float a = 0, b = 0, c = 0, d = 0;
+        cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[8]);
+        cudaEventElapsedTime(&b, ctx->ev[8], ctx->ev[9]);
+        cudaEventElapsedTime(&c, ctx->ev[9], ctx->ev[10]);
+        cudaEventElapsedTime(&d, ctx->ev[10], ctx->ev[11]);
+        stats->ms_zb_count += a;    // objects per zone
+        stats->ms_zb_scan += b;     // zone offsets
+        stats->ms_zb_scatter += c;  // records into zone buckets
+        stats->ms_zb_sort += d;     // in-zone sort + SoA output
+        stats->ms_build += a + b + c + d;
+        stats->n_launches += launches;
+    }
+    return XM_OK;
+}
+
+xm_status xm_build_impl(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_stats *stats)
+{
+    xm_ctx *ctx = seg->ctx;
+    if (n >= 0xFFFFFFF0ull) {
+        ctx->last_error = "segment larger than 2^32-16 records";
+        return XM_ERR_INVALID;
+    }
+    bool fallback = false;
+    XM_TRY(build_zones(seg, objs, n, stats, &fallback));
+    if (!fallback) return XM_OK;
+    return build_lsd(seg, objs, n, stats);
 }
 
 // ---------------------------------------------------------------------------
