@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--n", type=int, default=50_000_000, help="sources per catalog")
     ap.add_argument("--variant", default="filter32", choices=["filter32", "plain64"])
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--e2e-dist", action="store_true",
+                    help="e2e also returns distances (24-byte records instead of the reference's 16-byte pairs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
@@ -242,7 +244,7 @@ def run_ours(args):
         sa.rebuild_device(dA.data_ptr(), n, stats)
         sb.rebuild_device(dB.data_ptr(), n, stats)
         ms_ = ctx.match(sa, sb, r, flags, fetch=False)[2]
-        for k in ("ms_match", "n_tested", "n_exact", "n_border", "n_launches"):
+        for k in ("ms_match", "ms_plan", "n_tested", "n_exact", "n_border", "n_launches"):
             setattr(stats, k, getattr(stats, k) + ms_[k])
 
     for _ in range(args.warmup):
@@ -270,15 +272,19 @@ def run_ours(args):
         torch.distributed.barrier()
     K = args.steps
     per = {
-        "zb_count": stats.ms_zb_count / (2 * K), "zb_scan": stats.ms_zb_scan / (2 * K),
-        "zb_scatter": stats.ms_zb_scatter / (2 * K), "zb_sort_chunks": stats.ms_zb_sort / (2 * K),
-        "pair_kernel": stats.ms_match / K,
+        "zb_count": stats.ms_zb_count / (2 * K), "zb_offsets": stats.ms_zb_scan / (2 * K),
+        "zb_scatter": stats.ms_zb_scatter / (2 * K), "zb_zone_sort": stats.ms_zb_sort / (2 * K),
+        "pair_plan": stats.ms_plan / K, "pair_kernel": stats.ms_match / K,
     }
     kept_a, kept_b = len(sa), len(sb)
-    alg_bytes = {   # algorithmic bytes per launch
-        "zb_count": 24 * n, "zb_scatter": (24 + 32) * n, "zb_sort_chunks": (32 + 40) * n,
-        "zb_scan": 8 * int(np.ceil(180 / zh)),
-        "pair_kernel": 40 * kept_a + 40 * kept_b + 24 * n_match,
+    n_zones = int(np.ceil(180 / zh))
+    alg_bytes = {   # algorithmic bytes per launch (per catalog for the zb_* stages)
+        "zb_count": 24 * n,                        # records in
+        "zb_offsets": 16 * n_zones,                # counts in, offsets out, cursors
+        "zb_scatter": (24 + 32) * n,               # records in, 32-byte bucket records out
+        "zb_zone_sort": (32 + 64) * n,             # bucket records in; id, radec, xyz, xyz64 out
+        "pair_plan": 64 * int(np.ceil(len(sa) / 128)),   # one 64-byte plan per tile
+        "pair_kernel": 64 * kept_a + 64 * kept_b + 24 * n_match,   # both segments once, pairs out
     }
     peaks, peak_kind = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
@@ -289,7 +295,7 @@ def run_ours(args):
     dom = max(per, key=per.get)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": stages[dom]["GB/s"], "peak": hbm, "unit": "GB/s",
                 "frac": stages[dom]["frac"], "traffic": None, "peak_source": peak_kind}
-    pipeline_bytes = 64 * n * 2 + 24 * n_match
+    pipeline_bytes = 2 * (24 + 64) * n + 64 * (kept_a + kept_b) + 24 * n_match
     pipeline = {"alg_bytes": pipeline_bytes, "GB/s": pipeline_bytes / (ms * 1e-3) / 1e9,
                 "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / hbm}
     value = world * n_cand / (ms * 1e-3)
@@ -308,12 +314,21 @@ def run_ours(args):
     outP = hP.numpy().view(np.int64).reshape(-1, 2)
     outD = hD.numpy().view(np.float64)
 
+    e2e_parts = {"h2d": 0.0, "build": 0.0, "plan": 0.0, "match": 0.0, "d2h": 0.0}
+
     def e2e_step():
-        s1 = ctx.build(objA, zh, 0)
-        s2 = ctx.build(objB, zh, 1)
-        p, d, st = ctx.match(s1, s2, r, flags, out=(outP, outD))
+        bs = xm.XmStats()
+        s1 = ctx.build(objA, zh, 0, bs)
+        s2 = ctx.build(objB, zh, 1, bs)
+        p, d, st = ctx.match(s1, s2, r, flags, with_dist=args.e2e_dist,
+                             out=(outP, outD if args.e2e_dist else None))
         s1.free()
         s2.free()
+        e2e_parts["h2d"] += bs.ms_h2d
+        e2e_parts["build"] += bs.ms_build
+        e2e_parts["plan"] += st["ms_plan"]
+        e2e_parts["match"] += st["ms_match"]
+        e2e_parts["d2h"] += st["ms_d2h"]
         return len(p)
 
     e2e_step()
@@ -322,6 +337,8 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
+    for k in e2e_parts:
+        e2e_parts[k] = 0.0
     f0.record(stream)
     got = 0
     for _ in range(e2e_steps):
@@ -355,8 +372,11 @@ def run_ours(args):
         "roofline": roofline, "stages": stages, "pipeline_roofline": pipeline,
         "clocks": clocks,
         "e2e": {"value": world * n_cand / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 24 * n_match,
-                "path": "xm_segment_build(host) x2 + xm_match(host pairs + distances), pinned host buffers"},
+                "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": (24 if args.e2e_dist else 16) * n_match,
+                "path": "xm_segment_build(host) x2 + xm_match to host %s, pinned host buffers"
+                        % ("{idA, idB, dist} records" if args.e2e_dist else
+                           "{idA, idB} records (the reference's output record)"),
+                "parts_ms": {k: v / e2e_steps for k, v in e2e_parts.items()}},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(A, B, r, args.cpu_seconds)

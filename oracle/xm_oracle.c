@@ -484,14 +484,11 @@ static inline uint32_t or_raq32(double ra_rad)
     return (uint32_t)x;
 }
 
-/* raq bits kept in the sort key: whole 8-bit digits, >= 28 raq bits, <= 32 */
+/* raq bits kept in the sort key and in the segment (2^27 steps per turn) */
 int or_raq_bits(int64_t n_zones)
 {
-    int zb = 0;
-    for (uint64_t v = (uint64_t)n_zones; v; v >>= 1) ++zb;
-    int p = (zb + 28 + 7) / 8;
-    int rb = 8 * p - zb;
-    return rb < 32 ? rb : 32;
+    (void)n_zones;
+    return 27;
 }
 
 typedef struct {

@@ -12,9 +12,9 @@
 //   radec[n]               double2 radians, deg / RAD2DEG (Sorter.cu:52-62)
 //   xyz[n]                 float4: FP32 unit vector, w = raq bits
 //   xyz64[3n]              FP64 unit vector (the project sincos, Worker.cu:31-40)
-// zone = floor((dec + 90) / zh) (Sorter.cu:20-24); raq = the leading
-// raq_bits of floor(ra_rad * 2^31 / pi), a monotone quantisation of ra (its
-// step is 2 pi / 2^raq_bits, 2.3e-8 rad for raq_bits = 28), so within a zone
+// zone = floor((dec + 90) / zh) (Sorter.cu:20-24); raq = the leading 27
+// bits of floor(ra_rad * 2^31 / pi), a monotone quantisation of ra (its
+// step is 2 pi / 2^27, 4.7e-8 rad), so within a zone
 // the objects are sorted by ra up to that step and window searches on raq
 // give supersets of the RA windows.  (The reference sorts by (zone, ra) with
 // a comparison sort, Sorter.cu:27-43,153; the pair set does not depend on
@@ -44,6 +44,7 @@ constexpr int kRsThreads = 512;
 constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kTile = kRsThreads * kTileItems;   // 4096 keys
 constexpr int kMaxPasses = 8;
+constexpr int kRaqBits = 27;                  // raq bits kept; the 5 above carry the zone in a bucket
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
@@ -296,22 +297,34 @@ __global__ void zb_bounds_fill(const unsigned long long *__restrict__ keys, unsi
 }
 
 // ---------------------------------------------------------------------------
-// Zone-bucket build: objects counted per zone, the counts scanned into the
-// zone offsets, 32-byte records scattered into their zone's bucket through
-// per-zone atomic cursors, then every zone sorted in place by (raq, input
-// index) -- a warp per zone of up to kWarpZone objects (rank by counting), a
-// block per larger zone (bitonic sort in shared memory) up to kBlockZone.
+// Zone-bucket build.
+//   zc_count     objects per zone (and the populated range, dropped count)
+//   scan         zone offsets
+//   zc_classify  bucket cursors, list of zones above kWarpZone objects
+//   zc_scatter   32-byte records into buckets of 2^bucket_shift consecutive
+//                zones (per-bucket atomic cursors; few enough buckets that
+//                their write fronts stay in L2)
+//   zs_bucket    one block per bucket: records into zone order (shared-memory
+//                cursors, writes stay inside the bucket), then each zone of at
+//                most kWarpZone objects sorted by (raq, input index) by one
+//                warp and written out as the segment's SoA
+//   zs_block     zones of kWarpZone+1 .. kBlockZone objects: bitonic sort of a
+//                block
+// Zones above kBlockZone objects send the segment to the radix-sort build.
 // ---------------------------------------------------------------------------
 constexpr int kWarpZone = 256;
 constexpr int kBlockZone = 8192;
 constexpr int kZsThreads = 512;
+constexpr int kBucketMaxShift = 5;   // at most 32 zones per bucket
+constexpr int kBucketThreads = 256;
 
-struct ZRec {          // 32 bytes, one per kept object, in its zone's bucket
+struct ZRec {          // 32 bytes, one per kept object
     double ra, dec;    // radians
     long long id;
-    uint32_t raq;      // leading raq_bits of raq32(ra)
+    uint32_t raq;      // zone within its bucket << kRaqBits | leading kRaqBits of raq32(ra)
     uint32_t idx;      // input index
 };
+constexpr uint32_t kRaqMask = (1u << kRaqBits) - 1u;
 
 // Lanes whose value equals the previous lane's form runs (consecutive equal
 // zones, as in dec-ordered input); the run's first lane acts for the run.
@@ -335,6 +348,8 @@ __device__ __forceinline__ Run warp_run(int v, unsigned lane)
     return r;
 }
 
+constexpr int kScatterU = 4;   // records per lane per iteration (independent atomics in flight)
+
 // Pass 1: objects per zone; populated zone range and dropped count in misc.
 __global__ void zc_count(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp,
                          uint32_t *__restrict__ cnt, uint32_t *__restrict__ misc)
@@ -348,23 +363,31 @@ __global__ void zc_count(const xm_obj *__restrict__ objs, unsigned long long n, 
     __syncthreads();
     const unsigned lane = threadIdx.x & 31;
     unsigned zlo = 0xFFFFFFFFu, zhi = 0u, bad = 0u;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    const unsigned long long warp0 = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x * kScatterU;
+    const unsigned long long warp0 =
+        (((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull) * kScatterU;
     for (unsigned long long wb = warp0; wb < n; wb += stride) {
-        const unsigned long long i = wb + lane;
-        int z = -2;
-        if (i < n) {
-            const xm_obj o = objs[i];
-            z = isfinite(o.ra_deg) ? xm::zone_of(o.dec_deg, kp.zh_deg, kp.n_zones) : -1;
-            if (z < 0) {
-                ++bad;
-            } else {
-                zlo = min(zlo, (unsigned)z);
-                zhi = max(zhi, (unsigned)z);
+        int z[kScatterU];
+#pragma unroll
+        for (int u = 0; u < kScatterU; ++u) {
+            const unsigned long long i = wb + 32u * u + lane;
+            z[u] = -2;
+            if (i < n) {
+                const xm_obj o = objs[i];
+                z[u] = isfinite(o.ra_deg) ? xm::zone_of(o.dec_deg, kp.zh_deg, kp.n_zones) : -1;
             }
         }
-        const Run r = warp_run(z, lane);
-        if (r.is_head && z >= 0) atomicAdd(&cnt[z], r.len);
+#pragma unroll
+        for (int u = 0; u < kScatterU; ++u) {
+            if (z[u] == -1) {
+                ++bad;
+            } else if (z[u] >= 0) {
+                zlo = min(zlo, (unsigned)z[u]);
+                zhi = max(zhi, (unsigned)z[u]);
+            }
+            const Run r = warp_run(z[u], lane);
+            if (r.is_head && z[u] >= 0) atomicAdd(&cnt[z[u]], r.len);
+        }
     }
     zlo = __reduce_min_sync(0xffffffffu, zlo);
     zhi = __reduce_max_sync(0xffffffffu, zhi);
@@ -382,19 +405,20 @@ __global__ void zc_count(const xm_obj *__restrict__ objs, unsigned long long n, 
     }
 }
 
-// After the scan: cursor[z] = zone_off[z] (in place of the count), zones above
+// After the scan: bucket cursors bcur[b] = zone_off[b << shift], zones above
 // kWarpZone listed for the block sort, largest zone in misc[4], dropped count
 // stored beside the offsets (zone_off[n_zones + 1]).
-__global__ void zc_classify(uint32_t *__restrict__ cnt, uint32_t *__restrict__ zone_off, int n_zones,
-                            uint32_t *__restrict__ big, uint32_t *__restrict__ misc)
+__global__ void zc_classify(const uint32_t *__restrict__ cnt, uint32_t *__restrict__ zone_off, int n_zones,
+                            int shift, uint32_t *__restrict__ bcur, uint32_t *__restrict__ big,
+                            uint32_t *__restrict__ misc)
 {
     for (int z = blockIdx.x * blockDim.x + threadIdx.x; z <= n_zones; z += gridDim.x * blockDim.x) {
         if (z == n_zones) {
             zone_off[n_zones + 1] = misc[2];
             continue;
         }
+        if ((z & ((1 << shift) - 1)) == 0) bcur[z >> shift] = zone_off[z];
         const uint32_t m = cnt[z];
-        cnt[z] = zone_off[z];
         if (m > (uint32_t)kWarpZone) {
             big[atomicAdd(&misc[3], 1u)] = (uint32_t)z;
             atomicMax(&misc[4], m);
@@ -402,33 +426,52 @@ __global__ void zc_classify(uint32_t *__restrict__ cnt, uint32_t *__restrict__ z
     }
 }
 
-// Pass 2: every kept object's record into its zone bucket.
-__global__ void zc_scatter(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp,
-                           uint32_t *__restrict__ cursor, ZRec *__restrict__ recs)
+// Pass 2: every kept object's record into its bucket (unordered inside it).
+__global__ void zc_scatter(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp, int shift,
+                           uint32_t *__restrict__ bcur, ZRec *__restrict__ recs)
 {
     const unsigned lane = threadIdx.x & 31;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    const unsigned long long warp0 = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x * kScatterU;
+    const unsigned long long warp0 =
+        (((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull) * kScatterU;
     for (unsigned long long wb = warp0; wb < n; wb += stride) {
-        const unsigned long long i = wb + lane;
-        int z = -2;
-        xm_obj o;
-        if (i < n) {
-            o = objs[i];
-            z = isfinite(o.ra_deg) ? xm::zone_of(o.dec_deg, kp.zh_deg, kp.n_zones) : -1;
+        int bk[kScatterU];
+        uint32_t zl[kScatterU];
+        xm_obj o[kScatterU];
+#pragma unroll
+        for (int u = 0; u < kScatterU; ++u) {
+            const unsigned long long i = wb + 32u * u + lane;
+            bk[u] = -2;
+            zl[u] = 0;
+            if (i < n) {
+                o[u] = objs[i];
+                const int z = isfinite(o[u].ra_deg) ? xm::zone_of(o[u].dec_deg, kp.zh_deg, kp.n_zones) : -1;
+                bk[u] = z < 0 ? -1 : (z >> shift);
+                zl[u] = (uint32_t)z & ((1u << shift) - 1u);
+            }
         }
-        const Run r = warp_run(z, lane);
-        uint32_t base = 0;
-        if (r.is_head && z >= 0) base = atomicAdd(&cursor[z], r.len);
-        base = __shfl_sync(0xffffffffu, base, r.head);
-        if (z >= 0) {
-            const double ra = __ddiv_rn(o.ra_deg, XM_RAD2DEG);
-            const double dec = __ddiv_rn(o.dec_deg, XM_RAD2DEG);
-            ZRec *q = recs + base + (lane - r.head);
-            reinterpret_cast<double2 *>(q)[0] = make_double2(ra, dec);
-            reinterpret_cast<uint4 *>(q)[1] =
-                make_uint4((uint32_t)(unsigned long long)o.id, (uint32_t)((unsigned long long)o.id >> 32),
-                           xm::raq32(ra) >> kp.raq_shift, (uint32_t)i);
+        uint32_t base[kScatterU];
+        unsigned head[kScatterU];
+#pragma unroll
+        for (int u = 0; u < kScatterU; ++u) {
+            const Run r = warp_run(bk[u], lane);
+            head[u] = r.head;
+            base[u] = 0;
+            if (r.is_head && bk[u] >= 0) base[u] = atomicAdd(&bcur[bk[u]], r.len);
+        }
+#pragma unroll
+        for (int u = 0; u < kScatterU; ++u) {
+            const uint32_t b0 = __shfl_sync(0xffffffffu, base[u], head[u]);
+            if (bk[u] >= 0) {
+                const unsigned long long i = wb + 32u * u + lane;
+                const double ra = __ddiv_rn(o[u].ra_deg, XM_RAD2DEG);
+                const double dec = __ddiv_rn(o[u].dec_deg, XM_RAD2DEG);
+                ZRec *q = recs + b0 + (lane - head[u]);
+                reinterpret_cast<double2 *>(q)[0] = make_double2(ra, dec);
+                reinterpret_cast<uint4 *>(q)[1] =
+                    make_uint4((uint32_t)(unsigned long long)o[u].id, (uint32_t)((unsigned long long)o[u].id >> 32),
+                               zl[u] << kRaqBits | xm::raq32(ra) >> (32 - kRaqBits), (uint32_t)i);
+            }
         }
     }
 }
@@ -439,18 +482,6 @@ struct ZOut {
     float4 *xyz;
     double *xyz64;
 };
-
-__device__ __forceinline__ void zs_emit(const ZRec &r, unsigned long long j, const ZOut &o)
-{
-    double x, y, z;
-    xm::radec2xyz(r.ra, r.dec, x, y, z);
-    o.id[j] = r.id;
-    o.radec[j] = make_double2(r.ra, r.dec);
-    o.xyz[j] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z), __uint_as_float(r.raq));
-    o.xyz64[3 * j] = x;
-    o.xyz64[3 * j + 1] = y;
-    o.xyz64[3 * j + 2] = z;
-}
 
 __device__ __forceinline__ ZRec zs_load(const ZRec *p)
 {
@@ -465,56 +496,142 @@ __device__ __forceinline__ ZRec zs_load(const ZRec *p)
     return r;
 }
 
-template <int E>
-__device__ __forceinline__ void zs_warp_zone(const ZRec *__restrict__ recs, uint32_t b, uint32_t m,
-                                             unsigned long long *sk, unsigned lane, const ZOut &o)
+__device__ __forceinline__ void zs_emit(const ZRec &r, unsigned long long j, const ZOut &o)
 {
+    double x, y, z;
+    xm::radec2xyz(r.ra, r.dec, x, y, z);
+    o.id[j] = r.id;
+    o.radec[j] = make_double2(r.ra, r.dec);
+    o.xyz[j] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z),
+                           __uint_as_float(r.raq & kRaqMask));
+    o.xyz64[3 * j] = x;
+    o.xyz64[3 * j + 1] = y;
+    o.xyz64[3 * j + 2] = z;
+}
+
+// Per-warp scratch of the in-zone sort.
+struct WarpSort {
+    unsigned long long key[kWarpZone];   // (raq << 32 | idx), grouped by sub-range
+    uint16_t at[kWarpZone];              // record at each rank
+    uint32_t cnt[32], base[32];
+};
+
+// Sorts the m <= kWarpZone records zr[0..m) by (raq, idx) and writes them to
+// the outputs from position j0.  Keys are grouped by the top 5 raq bits
+// (32 sub-ranges of the turn), then ranked inside their group.
+template <int E>
+__device__ __forceinline__ void zs_sort_zone(const ZRec *zr, uint32_t m, unsigned long long j0, WarpSort &W,
+                                             unsigned lane, const ZOut &o)
+{
+    W.cnt[lane] = 0;
+    __syncwarp();
     unsigned long long key[E];
-    uint32_t rank[E];
+    uint32_t sub[E], slot[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const uint32_t k = lane + 32u * e;
         key[e] = ~0ull;
-        rank[e] = 0;
+        sub[e] = 0;
+        slot[e] = 0;
         if (k < m) {
-            const uint4 t = reinterpret_cast<const uint4 *>(recs + b + k)[1];
-            key[e] = ((unsigned long long)t.z << 32) | t.w;
-            sk[k] = key[e];
+            const uint4 t = reinterpret_cast<const uint4 *>(zr + k)[1];
+            const uint32_t raq = t.z & kRaqMask;
+            key[e] = ((unsigned long long)raq << 32) | t.w;
+            sub[e] = raq >> (kRaqBits - 5);
+            slot[e] = atomicAdd(&W.cnt[sub[e]], 1u);
         }
     }
     __syncwarp();
-    for (uint32_t j = 0; j < m; ++j) {
-        const unsigned long long kj = sk[j];
+    const uint32_t c = W.cnt[lane];
+    uint32_t incl = c;
 #pragma unroll
-        for (int e = 0; e < E; ++e) rank[e] += kj < key[e] ? 1u : 0u;
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= (unsigned)d) incl += y;
     }
+    W.base[lane] = incl - c;
+    __syncwarp();
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const uint32_t k = lane + 32u * e;
-        if (k < m) zs_emit(zs_load(recs + b + k), (unsigned long long)b + rank[e], o);
+        if (k < m) {
+            const uint32_t p = W.base[sub[e]] + slot[e];
+            W.key[p] = key[e];
+        }
+    }
+    __syncwarp();
+    uint32_t rank[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t k = lane + 32u * e;
+        rank[e] = 0;
+        if (k < m) {
+            const uint32_t b0 = W.base[sub[e]], b1 = b0 + W.cnt[sub[e]];
+            uint32_t r = b0;
+            for (uint32_t q = b0; q < b1; ++q) r += W.key[q] < key[e] ? 1u : 0u;
+            rank[e] = r;
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t k = lane + 32u * e;
+        if (k < m) W.at[rank[e]] = (uint16_t)k;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t p = lane + 32u * e;
+        if (p < m) zs_emit(zs_load(zr + W.at[p]), j0 + p, o);
     }
     __syncwarp();
 }
 
-// Zones of at most kWarpZone objects: one warp each, ranks by counting
-// (keys are unique: the input index is part of the key).
-__global__ void __launch_bounds__(256)
-zs_warp(const ZRec *__restrict__ recs, const uint32_t *__restrict__ zone_off, int n_zones, ZOut o)
+// One block per bucket: records into zone order inside the bucket (recs_z),
+// then the zones of at most kWarpZone objects sorted and written out.
+__global__ void __launch_bounds__(kBucketThreads)
+zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint32_t *__restrict__ zone_off,
+          int n_zones, int shift, int n_buckets, KeyParams kp, ZOut o, uint32_t *__restrict__ misc)
 {
-    __shared__ unsigned long long skeys[8][kWarpZone];
+    constexpr int kW = kBucketThreads / 32;
+    __shared__ uint32_t cur[1 << kBucketMaxShift];
+    __shared__ WarpSort ws[kW];
     const unsigned lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;
-    unsigned long long *sk = skeys[w];
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int z = gw; z < n_zones; z += nw) {
-        const uint32_t b = zone_off[z];
-        const uint32_t m = zone_off[z + 1] - b;
-        if (m == 0 || m > (uint32_t)kWarpZone) continue;
-        if (m <= 32) zs_warp_zone<1>(recs, b, m, sk, lane, o);
-        else if (m <= 64) zs_warp_zone<2>(recs, b, m, sk, lane, o);
-        else if (m <= 128) zs_warp_zone<4>(recs, b, m, sk, lane, o);
-        else zs_warp_zone<8>(recs, b, m, sk, lane, o);
+    const int warp = threadIdx.x >> 5;
+    for (int bk = blockIdx.x; bk < n_buckets; bk += gridDim.x) {
+        const int z0 = bk << shift;
+        const int nzb = min(1 << shift, n_zones - z0);
+        const uint32_t r0 = zone_off[z0], r1 = zone_off[z0 + nzb];
+        if (threadIdx.x < nzb) cur[threadIdx.x] = zone_off[z0 + threadIdx.x];
+        __syncthreads();
+        if (nzb == 1) {
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) recs_z[i] = recs_b[i];
+        } else {
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const double2 a = reinterpret_cast<const double2 *>(recs_b + i)[0];
+                const uint4 t = reinterpret_cast<const uint4 *>(recs_b + i)[1];
+                const uint32_t zl = t.z >> kRaqBits;
+                if (zl >= (uint32_t)nzb) {   // cannot happen: written by zc_scatter for this bucket
+                    atomicOr(&misc[5], 1u);
+                    continue;
+                }
+                const uint32_t p = atomicAdd(&cur[zl], 1u);
+                reinterpret_cast<double2 *>(recs_z + p)[0] = a;
+                reinterpret_cast<uint4 *>(recs_z + p)[1] = t;
+            }
+        }
+        __syncthreads();
+        for (int k = warp; k < nzb; k += kW) {
+            const uint32_t b = zone_off[z0 + k];
+            const uint32_t m = zone_off[z0 + k + 1] - b;
+            if (m == 0 || m > (uint32_t)kWarpZone) continue;
+            const ZRec *zr = recs_z + b;
+            if (m <= 32) zs_sort_zone<1>(zr, m, b, ws[warp], lane, o);
+            else if (m <= 64) zs_sort_zone<2>(zr, m, b, ws[warp], lane, o);
+            else if (m <= 128) zs_sort_zone<4>(zr, m, b, ws[warp], lane, o);
+            else zs_sort_zone<8>(zr, m, b, ws[warp], lane, o);
+        }
+        __syncthreads();
     }
 }
 
@@ -539,7 +656,7 @@ zs_block(const ZRec *__restrict__ recs, const uint32_t *__restrict__ zone_off, c
             unsigned long long key = ~0ull;
             if (k < m) {
                 const uint4 t = reinterpret_cast<const uint4 *>(recs + b + k)[1];
-                key = ((unsigned long long)t.z << 32) | t.w;
+                key = ((unsigned long long)(t.z & kRaqMask) << 32) | t.w;
             }
             sk[k] = key;
             sp[k] = (uint16_t)k;
@@ -589,14 +706,13 @@ int bit_width(uint64_t v)
 
 }  // namespace
 
-// Bits of the quantised ra kept in the sort key: enough for the key to fill
-// whole 8-bit digits with at least 28 raq bits, at most 32.
+// Bits of the quantised ra kept in the segment (xyz.w) and in the sort key:
+// kRaqBits (2^27 steps per turn, 4.7e-8 rad); radix passes over zone and raq.
 void xm_raq_layout(int32_t n_zones, int *raq_bits, int *passes)
 {
     const int zb = bit_width((uint64_t)n_zones);   // zone values 0..n_zones (n_zones = dropped)
-    const int p = (zb + 28 + 7) / 8;
-    *passes = p;
-    *raq_bits = std::min(32, 8 * p - zb);
+    *passes = (zb + kRaqBits + 7) / 8;
+    *raq_bits = kRaqBits;
 }
 
 static xm_status ensure(xm_ctx *ctx, void **p, size_t *have, size_t need)
@@ -782,18 +898,26 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     seg->raq_bits = raq_bits;
     XM_TRY(seg_storage(seg, n));
     const uint64_t nn = std::max<uint64_t>(n, 1);
-    // scratch: records, per-zone counts/cursors, big-zone list, scan scratch, misc
+    // buckets of 2^shift zones, at least 4 per SM
+    int shift = kBucketMaxShift;
+    while (shift > 0 && (nz >> shift) < ctx->sm_count * 4) --shift;
+    const int n_buckets = (nz + (1 << shift) - 1) >> shift;
+    // scratch: records by bucket and by zone, per-zone counts, bucket cursors,
+    // big-zone list, scan scratch, misc
     const size_t rb = (nn * sizeof(ZRec) + 255) & ~(size_t)255;
     const size_t zb = (((size_t)nz + 1) * 4 + 255) & ~(size_t)255;
+    const size_t bb = (((size_t)n_buckets + 1) * 4 + 255) & ~(size_t)255;
     const size_t sb = (xm_scan_tmp_bytes((size_t)nz) + 255) & ~(size_t)255;
     const size_t mb = 256;
-    XM_TRY(ensure(ctx, &seg->tmp, &seg->tmp_bytes, rb + 2 * zb + sb + mb));
+    XM_TRY(ensure(ctx, &seg->tmp, &seg->tmp_bytes, 2 * rb + 2 * zb + bb + sb + mb));
     char *w = (char *)seg->tmp;
-    ZRec *recs = (ZRec *)w; w += rb;
+    ZRec *recs_b = (ZRec *)w; w += rb;
+    ZRec *recs_z = (ZRec *)w; w += rb;
     uint32_t *cnt = (uint32_t *)w; w += zb;
     uint32_t *big = (uint32_t *)w; w += zb;
+    uint32_t *bcur = (uint32_t *)w; w += bb;
     void *scan_tmp = w; w += sb;
-    uint32_t *misc = (uint32_t *)w;   // z_lo, z_hi, dropped, n_big, largest zone
+    uint32_t *misc = (uint32_t *)w;   // z_lo, z_hi, dropped, n_big, largest zone, error
     uint32_t launches = 0;
 
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[0], st));
@@ -802,29 +926,33 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     XM_CUDA(ctx, cudaMemsetAsync(misc, 0xFF, 4, st));
     KeyParams kp{seg->zh_deg, nz, 32 - raq_bits, raq_bits, passes};
     if (n > 0) {
-        zc_count<<<grid_for(n, 256, ctx->sm_count, 8), 256, 0, st>>>(objs, n, kp, cnt, misc);
+        zc_count<<<grid_for((n + kScatterU - 1) / kScatterU, 256, ctx->sm_count, 8), 256, 0, st>>>(objs, n, kp, cnt,
+                                                                                                   misc);
         launches++;
     }
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[8], st));
     XM_CUDA(ctx, xm_scan_exclusive_u32(cnt, seg->zone_off, (size_t)nz, scan_tmp, st));
-    zc_classify<<<grid_for((uint64_t)nz + 1, 256, ctx->sm_count, 8), 256, 0, st>>>(cnt, seg->zone_off, nz, big, misc);
+    zc_classify<<<grid_for((uint64_t)nz + 1, 256, ctx->sm_count, 8), 256, 0, st>>>(cnt, seg->zone_off, nz, shift,
+                                                                                     bcur, big, misc);
     launches += 4;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[9], st));
     if (n > 0) {
-        zc_scatter<<<grid_for(n, 256, ctx->sm_count, 8), 256, 0, st>>>(objs, n, kp, cnt, recs);
+        zc_scatter<<<grid_for((n + kScatterU - 1) / kScatterU, 256, ctx->sm_count, 8), 256, 0, st>>>(
+            objs, n, kp, shift, bcur, recs_b);
         launches++;
     }
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[10], st));
     ZOut o{(long long *)seg->id, seg->radec, seg->xyz, seg->xyz64};
     if (n > 0) {
-        zs_warp<<<grid_for((uint64_t)nz * 32, 256, ctx->sm_count, 8), 256, 0, st>>>(recs, seg->zone_off, nz, o);
+        zs_bucket<<<std::min(n_buckets, ctx->sm_count * 8), kBucketThreads, 0, st>>>(
+            recs_b, recs_z, seg->zone_off, nz, shift, n_buckets, kp, o, misc);
         static bool attr = false;
         const size_t smem = (size_t)kBlockZone * 10;
         if (!attr) {
             XM_CUDA(ctx, cudaFuncSetAttribute(zs_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr = true;
         }
-        zs_block<<<ctx->sm_count * 2, kZsThreads, smem, st>>>(recs, seg->zone_off, big, misc, o);
+        zs_block<<<ctx->sm_count * 2, kZsThreads, smem, st>>>(recs_z, seg->zone_off, big, misc, o);
         launches += 2;
     }
     XM_CUDA(ctx, cudaGetLastError());
@@ -842,6 +970,10 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     } else {
         seg->z_lo = 0;
         seg->z_hi = -1;
+    }
+    if (hm[5]) {
+        ctx->last_error = "zone build: a record left its bucket";
+        return XM_ERR_CUDA;
     }
     if (hm[4] > (uint32_t)kBlockZone) *fallback = true;
     if (stats) {

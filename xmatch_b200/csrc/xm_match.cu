@@ -588,6 +588,15 @@ struct __align__(16) TilePlan {    // 64 bytes
 };
 static_assert(sizeof(TilePlan) == 64, "plan layout");
 
+__device__ __forceinline__ void store_plan(TilePlan *dst, const TilePlan &P)
+{
+    uint4 *d = reinterpret_cast<uint4 *>(dst);
+    d[0] = make_uint4(P.a_start, P.a_len, P.mode, (uint32_t)P.zf);
+    d[1] = make_uint4((uint32_t)P.band_lo, P.job, P.b_start, P.b_len);
+    d[2] = make_uint4(P.seg_g[0], P.seg_g[1], P.seg_g[2], P.seg_g[3]);
+    d[3] = make_uint4(P.seg_len[0], P.seg_len[1], P.seg_len[2], P.seg_len[3]);
+}
+
 // Cuts work item `item` into tiles (see the file header); calls f(start, len, zf, zl).
 template <class F>
 __device__ __forceinline__ void for_each_tile(const JobDev &J, uint32_t item, uint32_t zc, uint32_t tile, F f)
@@ -711,7 +720,7 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
                 P.b_start = B0 + q * piece;
                 P.b_len = min(piece, B1 - P.b_start);
                 P.mode = PLAN_WHOLE | zword;
-                if (oh < max_tiles) plans[oh] = P;
+                if (oh < max_tiles) store_plan(plans + oh, P);
                 else atomicExch(err, 1ull);
                 ++oh;
             }
@@ -732,7 +741,9 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
             const uint32_t t_hi2 = xm::raq32(ra_l + alpha + 2 * kWinEps - XM_TWO_PI) >> sh;
             const uint32_t t_lo3 = xm::raq32(ra_f - alpha - 2 * kWinEps + XM_TWO_PI) >> sh;
             uint32_t total = 0;
-            for (int k = 0; k < (int)nseg; ++k) {
+#pragma unroll
+            for (int k = 0; k < kMaxPlanSeg; ++k) {
+                if (k >= (int)nseg) break;
                 const uint32_t b0 = J.b_zoff[band_lo + k], b1 = J.b_zoff[band_lo + k + 1];
                 uint32_t sb = b0, ln = b1 - b0;
                 if (ln > 0) {
@@ -753,7 +764,7 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
         }
         // nseg is only read for WHOLE (<= kMaxBand) and UNION (<= kMaxPlanSeg) plans
         P.mode = mode | zword;
-        if (o < max_tiles) plans[o] = P;
+        if (o < max_tiles) store_plan(plans + o, P);
         else atomicExch(err, 1ull);
         ++o;
     });
