@@ -1,6 +1,6 @@
 """ctypes declarations of include/xmatch.h (libxmatch_b200.so).
 
-The shared library is built in-tree (``python -m xmatch_b200.build``).  There
+The shared library is built in-tree (``python xmatch_b200/build.py``).  There
 is no fallback: if the library is missing or cannot be loaded, import of
 this module raises.
 """
@@ -105,7 +105,7 @@ SIGNATURES = {
 
 def load(path=LIB_PATH):
     if not os.path.exists(path):
-        raise ImportError("libxmatch_b200.so not built: run `python -m xmatch_b200.build` (%s)" % path)
+        raise ImportError("libxmatch_b200.so not built: run `python xmatch_b200/build.py` (%s)" % path)
     lib = ctypes.CDLL(path)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)

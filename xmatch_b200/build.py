@@ -1,6 +1,6 @@
 """Build libxmatch_b200.so (sm_100a) in-tree.
 
-    python -m xmatch_b200.build          # or: python xmatch_b200/build.py
+    python xmatch_b200/build.py         # (the package itself needs the library to import)
 
 Every CUDA source is compiled for sm_100a only; host code is compiled with
 -ffp-contract=off so host-side FP64 formulas (RA half-width, thresholds)
