@@ -314,16 +314,26 @@ def run_ours(args):
     outP = hP.numpy().view(np.int64).reshape(-1, 2)
     outD = hD.numpy().view(np.float64)
 
-    e2e_parts = {"h2d": 0.0, "build": 0.0, "plan": 0.0, "match": 0.0, "d2h": 0.0}
+    e2e_parts = {"h2d": 0.0, "build": 0.0, "plan": 0.0, "match": 0.0, "d2h": 0.0,
+                 "wall_build_a": 0.0, "wall_build_b": 0.0, "wall_match": 0.0, "wall_free": 0.0}
 
     def e2e_step():
         bs = xm.XmStats()
+        t0 = time.perf_counter()
         s1 = ctx.build(objA, zh, 0, bs)
+        t1 = time.perf_counter()
         s2 = ctx.build(objB, zh, 1, bs)
+        t2 = time.perf_counter()
         p, d, st = ctx.match(s1, s2, r, flags, with_dist=args.e2e_dist,
                              out=(outP, outD if args.e2e_dist else None))
+        t3 = time.perf_counter()
         s1.free()
         s2.free()
+        t4 = time.perf_counter()
+        e2e_parts["wall_build_a"] += (t1 - t0) * 1e3
+        e2e_parts["wall_build_b"] += (t2 - t1) * 1e3
+        e2e_parts["wall_match"] += (t3 - t2) * 1e3
+        e2e_parts["wall_free"] += (t4 - t3) * 1e3
         e2e_parts["h2d"] += bs.ms_h2d
         e2e_parts["build"] += bs.ms_build
         e2e_parts["plan"] += st["ms_plan"]

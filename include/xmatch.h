@@ -54,7 +54,8 @@ enum {
                                  every surviving pair decided by the FP64 predicate */
     XM_PLAIN64 = 1u << 0,     /* all-FP64: FP64 cuts, unit vectors by sincos per pair */
     XM_COUNT_CAND = 1u << 1,  /* also count reference-prefilter candidates (stats.n_cand) */
-    XM_NO_DIST = 1u << 2      /* do not compute distances (16-byte output) */
+    XM_NO_DIST = 1u << 2,     /* do not compute distances (16-byte output) */
+    XM_NO_GRAPH = 1u << 3     /* launch the match kernels directly, not through the context's CUDA graph */
 };
 
 /* Stats may be NULL everywhere; when given, the call accumulates into it. */

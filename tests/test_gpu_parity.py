@@ -255,6 +255,38 @@ def test_batch_equals_single_jobs(ctx, fixtures):
         b.free()
 
 
+def test_graph_and_direct_launches_agree(ctx, fixtures):
+    # the match sequence runs as the context's CUDA graph unless XM_NO_GRAPH; a
+    # second shape (other radius) exercises the graph update
+    import xmatch_b200 as xm
+    a, a2 = fixtures
+    for r in (5, 20, 5):
+        pg, dg, sg = run_gpu(ctx, a2, a, r, flags=0)
+        pd, dd, sd = run_gpu(ctx, a2, a, r, flags=xm.XM_NO_GRAPH)
+        pg, dg = sp(pg, dg)
+        pd, dd = sp(pd, dd)
+        assert np.array_equal(pg, pd) and dg.tobytes() == dd.tobytes()
+        assert sg["n_cand"] == sd["n_cand"] and sg["n_tested"] == sd["n_tested"]
+
+
+def test_batch_of_many_radii(ctx):
+    # 200 jobs, each with its own radius and zone height: one alpha table per
+    # job's zone range, one launch
+    from xmatch_b200 import synth
+    jobs = synth.config2_jobs(n_jobs=200, seed=11, scale=0.02)
+    segs = [(ctx.build(A, r * ARCSEC), ctx.build(B, r * ARCSEC), r * ARCSEC) for A, B, r in jobs]
+    res, cnt, st = ctx.match_batch(segs)
+    for k, (A, B, r) in enumerate(jobs):
+        po, do, _ = oracle.xmatch(A, B, r * ARCSEC)
+        p, d = sp(*res[k])
+        po, do = sp(po, do)
+        assert cnt[k] == len(po) and np.array_equal(p, po), k
+        assert np.max(np.abs(d - do), initial=0) <= DIST_TOL
+    for x, y, _ in segs:
+        x.free()
+        y.free()
+
+
 def test_segmentation_invariance(ctx, fixtures):
     a, _ = fixtures
     whole, _, _ = oracle.xmatch(a, a, 5 * ARCSEC)

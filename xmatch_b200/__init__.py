@@ -12,7 +12,7 @@ import ctypes
 import numpy as np
 
 from . import _capi
-from ._capi import (XM_COUNT_CAND, XM_FILTER32, XM_NO_DIST, XM_OK, XM_PLAIN64,  # noqa: F401
+from ._capi import (XM_COUNT_CAND, XM_FILTER32, XM_NO_DIST, XM_NO_GRAPH, XM_OK, XM_PLAIN64,  # noqa: F401
                     XmJob, XmPairs, XmStats, XmTuning)
 
 OBJ_DTYPE = np.dtype([("id", "<i8"), ("ra", "<f8"), ("dec", "<f8")])   # Obj.h:21-25, 24 bytes

@@ -27,6 +27,7 @@ XM_FILTER32 = 0
 XM_PLAIN64 = 1 << 0
 XM_COUNT_CAND = 1 << 1
 XM_NO_DIST = 1 << 2
+XM_NO_GRAPH = 1 << 3
 
 
 class XmObj(ctypes.Structure):

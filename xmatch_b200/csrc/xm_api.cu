@@ -7,6 +7,7 @@
 // queued on the context's stream, and results are copied back only when the
 // caller asks for them.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -200,14 +201,17 @@ extern "C" xm_status xm_ctx_destroy(xm_ctx *ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     free_result(ctx);
-    for (auto &kv : ctx->alpha_cache) xm_dev_free(ctx, kv.second.dev);
+    alpha_cache_clear(ctx);
     xm_dev_free(ctx, ctx->d_jobs);
     xm_dev_free(ctx, ctx->d_work);
     xm_dev_free(ctx, ctx->d_plans);
+    xm_dev_free(ctx, ctx->build_tmp);
+    xm_dev_free(ctx, ctx->stage);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->counters) cudaFree(ctx->counters);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
     if (ctx->h_tiles) cudaFreeHost(ctx->h_tiles);
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     for (auto &ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
@@ -244,36 +248,100 @@ extern "C" xm_status xm_ctx_synchronize(xm_ctx *ctx)
     return XM_OK;
 }
 
-xm_status xm_get_alpha(xm_ctx *ctx, double sr_deg, double zh_deg, int32_t n_zones, const double **dev_alpha)
+static constexpr size_t kAlphaCacheBytes = 512ull << 20;   // cached tables per context, at most
+
+static xm_alpha_key alpha_key(const xm_alpha_req &r)
 {
-    uint64_t a, b;
-    std::memcpy(&a, &sr_deg, 8);
-    std::memcpy(&b, &zh_deg, 8);
-    uint64_t key = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull + (a << 6) + (a >> 2));
-    auto it = ctx->alpha_cache.find(key);
-    if (it != ctx->alpha_cache.end() && it->second.n_zones == n_zones) {
-        *dev_alpha = it->second.dev;
-        return XM_OK;
+    xm_alpha_key k;
+    std::memcpy(&k.sr, &r.sr_deg, 8);
+    std::memcpy(&k.zh, &r.zh_deg, 8);
+    k.z0 = r.z0;
+    k.z1 = r.z1;
+    return k;
+}
+
+void alpha_cache_clear(xm_ctx *ctx)
+{
+    for (auto &kv : ctx->alpha_cache) xm_dev_free(ctx, kv.second.dev);
+    ctx->alpha_cache.clear();
+    ctx->alpha_bytes = 0;
+}
+
+// Tables missing from the cache are computed on the host (libm, as the
+// reference does), all of them together over a pool of threads in chunks of
+// zones, then copied to the device.
+xm_status xm_get_alpha_ranges(xm_ctx *ctx, xm_alpha_req *req, size_t n)
+{
+    std::vector<xm_alpha_key> miss;
+    size_t miss_bytes = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const xm_alpha_key k = alpha_key(req[i]);
+        if (ctx->alpha_cache.count(k)) continue;
+        bool dup = false;
+        for (size_t j = 0; j < miss.size() && !dup; ++j)   // few misses per call in practice
+            dup = !(miss[j] < k) && !(k < miss[j]);
+        if (dup) continue;
+        miss.push_back(k);
+        miss_bytes += (size_t)(k.z1 - k.z0 + 1) * 8;
     }
-    if (ctx->alpha_cache.size() > 64) {
-        for (auto &kv : ctx->alpha_cache) xm_dev_free(ctx, kv.second.dev);
-        ctx->alpha_cache.clear();
+    if (!miss.empty() && ctx->alpha_bytes + miss_bytes > kAlphaCacheBytes) {
+        alpha_cache_clear(ctx);
+        miss.clear();
+        miss_bytes = 0;
+        for (size_t i = 0; i < n; ++i) {
+            const xm_alpha_key k = alpha_key(req[i]);
+            bool dup = false;
+            for (size_t j = 0; j < miss.size() && !dup; ++j) dup = !(miss[j] < k) && !(k < miss[j]);
+            if (dup) continue;
+            miss.push_back(k);
+            miss_bytes += (size_t)(k.z1 - k.z0 + 1) * 8;
+        }
     }
-    std::vector<double> h((size_t)n_zones);
-    xm_host_alpha_table(sr_deg, zh_deg, n_zones, h.data());
-    xm_alpha_entry e;
-    e.n_zones = n_zones;
-    XM_TRY(xm_dev_alloc(ctx, (void **)&e.dev, (size_t)n_zones * 8));
-    XM_CUDA(ctx, cudaMemcpyAsync(e.dev, h.data(), (size_t)n_zones * 8, cudaMemcpyHostToDevice, ctx->stream));
-    XM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // h goes out of scope
-    ctx->alpha_cache[key] = e;
-    *dev_alpha = e.dev;
+    if (!miss.empty()) {
+        std::vector<size_t> off(miss.size() + 1, 0);
+        for (size_t j = 0; j < miss.size(); ++j) off[j + 1] = off[j] + (size_t)(miss[j].z1 - miss[j].z0 + 1);
+        std::vector<double> h(off.back());
+        // tasks: (table, first zone) chunks of at most 8192 zones
+        struct Task { size_t t; int32_t za, zb; };
+        std::vector<Task> tasks;
+        for (size_t j = 0; j < miss.size(); ++j)
+            for (int64_t z = miss[j].z0; z <= miss[j].z1; z += 8192)
+                tasks.push_back({j, (int32_t)z, (int32_t)std::min<int64_t>(z + 8191, miss[j].z1)});
+        std::atomic<size_t> next{0};
+        auto work = [&]() {
+            for (size_t q; (q = next.fetch_add(1)) < tasks.size();) {
+                const Task &T = tasks[q];
+                double sr, zh;
+                std::memcpy(&sr, &miss[T.t].sr, 8);
+                std::memcpy(&zh, &miss[T.t].zh, 8);
+                double *dst = h.data() + off[T.t] - miss[T.t].z0;
+                for (int32_t z = T.za; z <= T.zb; ++z) dst[z] = calc_alpha_zone(sr, zh, z);
+            }
+        };
+        const unsigned nt = (unsigned)std::min<size_t>(tasks.size(),
+                                                       std::max(1u, std::min(32u, std::thread::hardware_concurrency())));
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < nt; ++t) th.emplace_back(work);
+        work();
+        for (auto &x : th) x.join();
+        for (size_t j = 0; j < miss.size(); ++j) {
+            xm_alpha_entry e;
+            e.bytes = (off[j + 1] - off[j]) * 8;
+            XM_TRY(xm_dev_alloc(ctx, (void **)&e.dev, e.bytes));
+            XM_CUDA(ctx, cudaMemcpyAsync(e.dev, h.data() + off[j], e.bytes, cudaMemcpyHostToDevice, ctx->stream));
+            ctx->alpha_cache[miss[j]] = e;
+            ctx->alpha_bytes += e.bytes;
+        }
+        XM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // h goes out of scope
+    }
+    for (size_t i = 0; i < n; ++i) req[i].dev = ctx->alpha_cache.at(alpha_key(req[i])).dev;
     return XM_OK;
 }
 
 // ---------------------------------------------------------------------------
 // segments
 // ---------------------------------------------------------------------------
+
 static xm_status new_segment(xm_ctx *ctx, uint32_t seg_id, double zh_deg, xm_segment **out)
 {
     if (!(zh_deg > 0) || !std::isfinite(zh_deg)) return XM_ERR_INVALID;
@@ -324,8 +392,17 @@ extern "C" xm_status xm_segment_build(xm_ctx *ctx, uint32_t seg_id, const xm_obj
     cudaSetDevice(ctx->device);
     xm_segment *s = nullptr;
     XM_TRY(new_segment(ctx, seg_id, zh_deg, &s));
-    void *d = nullptr;
-    xm_status rc = xm_dev_alloc(ctx, &d, std::max<uint64_t>(n, 1) * sizeof(xm_obj));
+    // host records land in the context's staging buffer (grown, never shrunk)
+    xm_status rc = XM_OK;
+    const size_t need = std::max<uint64_t>(n, 1) * sizeof(xm_obj);
+    if (ctx->stage_bytes < need) {
+        xm_dev_free(ctx, ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_bytes = 0;
+        rc = xm_dev_alloc(ctx, &ctx->stage, need);
+        if (rc == XM_OK) ctx->stage_bytes = need;
+    }
+    void *d = ctx->stage;
     if (rc == XM_OK && n) {
         if (stats) cudaEventRecord(ctx->ev[12], ctx->stream);
         cudaError_t e = cudaMemcpyAsync(d, host_objs, n * sizeof(xm_obj), cudaMemcpyHostToDevice, ctx->stream);
@@ -341,7 +418,6 @@ extern "C" xm_status xm_segment_build(xm_ctx *ctx, uint32_t seg_id, const xm_obj
         cudaEventElapsedTime(&ms, ctx->ev[12], ctx->ev[13]);   // build_impl synchronised the stream
         stats->ms_h2d += ms;
     }
-    xm_dev_free(ctx, d);
     if (rc != XM_OK) {
         xm_segment_free(s);
         return rc;
@@ -355,12 +431,7 @@ extern "C" xm_status xm_segment_free(xm_segment *seg)
     if (!seg) return XM_OK;
     xm_ctx *ctx = seg->ctx;
     cudaSetDevice(ctx->device);
-    xm_dev_free(ctx, seg->zone_off);
-    xm_dev_free(ctx, seg->id);
-    xm_dev_free(ctx, seg->radec);
-    xm_dev_free(ctx, seg->xyz);
-    xm_dev_free(ctx, seg->xyz64);
-    xm_dev_free(ctx, seg->tmp);
+    xm_dev_free(ctx, seg->store);
     delete seg;
     return XM_OK;
 }
@@ -429,6 +500,8 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
 {
     P.jobs.resize(n_jobs);
     uint64_t items = 0, guess = 0;
+    std::vector<xm_alpha_req> areq;   // RA half-widths of every job's A zones
+    std::vector<uint32_t> ajob;
     for (uint32_t j = 0; j < n_jobs; ++j) {
         const xm_segment *A = jobs[j].A, *B = jobs[j].B;
         if (!A || !B || A->ctx != ctx || B->ctx != ctx) {
@@ -444,8 +517,6 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
             ctx->last_error = "job " + std::to_string(j) + ": invalid radius";
             return XM_ERR_INVALID;
         }
-        const double *alpha = nullptr;
-        XM_TRY(xm_get_alpha(ctx, p.sr_deg, A->zh_deg, A->n_zones, &alpha));
         xm::JobDev &d = P.jobs[j];
         std::memset(&d, 0, sizeof(d));
         d.a_id = (const long long *)A->id;
@@ -458,7 +529,6 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
         d.b_xyz = B->xyz;
         d.b_xyz64 = B->xyz64;
         d.b_zoff = B->zone_off;
-        d.alpha = alpha;
         d.sr_rad = p.sr_rad;
         d.sr_dist2 = p.sr_dist2;
         d.thr_hi = p.thr_hi;
@@ -472,12 +542,19 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
         d.item_begin = (uint32_t)items;
         if (A->n > 0 && B->n > 0 && A->z_hi >= A->z_lo) {
             items += ((uint64_t)(A->z_hi - A->z_lo) + zc) / zc;
+            areq.push_back({p.sr_deg, A->zh_deg, A->z_lo, A->z_hi, nullptr});
+            ajob.push_back(j);
         }
         guess += 2 * std::max(A->n, B->n);   // Worker.cu:296-297 default
         if (items >= 0xFFFFFF00ull) {
             ctx->last_error = "too many work items in one launch";
             return XM_ERR_INVALID;
         }
+    }
+    XM_TRY(xm_get_alpha_ranges(ctx, areq.data(), areq.size()));
+    for (size_t q = 0; q < areq.size(); ++q) {
+        P.jobs[ajob[q]].alpha = areq[q].dev;
+        P.jobs[ajob[q]].alpha_z0 = areq[q].z0;
     }
     P.n_items = (uint32_t)items;
     P.cap_guess = std::max<uint64_t>(guess, 1 << 16);
@@ -558,23 +635,53 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
     }
     uint32_t retries = 0;
     float ms = 0, plan_ms = 0;
+    const bool use_graph = (flags & XM_NO_GRAPH) == 0;
     for (;;) {
-        XM_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16 * sizeof(unsigned long long), st));
         xm::MatchOut out;
         out.pairs = (long long *)ctx->res.pairs;
         out.dist = L.dist ? ctx->res.dist : nullptr;
         out.job = want_job ? ctx->res.job : nullptr;
         out.cap = ctx->res.cap;
         out.counters = ctx->counters;
-        if (P.n_items > 0 && retries == 0)
-            XM_CUDA(ctx, xm::plan_make(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_items, tile_off, n_normal,
-                                       n_heavy, ctx->d_plans, ctx->counters + 7, st));
-        XM_CUDA(ctx, cudaEventRecord(ctx->ev[2], st));
-        if (P.n_items > 0)
-            XM_CUDA(ctx, xm::run_pairs(L, (const xm::JobDev *)ctx->d_jobs, ctx->d_plans, n_normal, n_heavy, out, st));
-        XM_CUDA(ctx, cudaEventRecord(ctx->ev[3], st));
-        XM_CUDA(ctx, cudaMemcpyAsync(ctx->h_counters, ctx->counters, 16 * sizeof(unsigned long long),
-                                     cudaMemcpyDeviceToHost, st));
+        // counters cleared, tile plans, pair kernel, counters read back
+        auto enqueue = [&](unsigned ev_flags) -> cudaError_t {
+            cudaError_t e = cudaMemsetAsync(ctx->counters, 0, 16 * sizeof(unsigned long long), st);
+            if (e == cudaSuccess && P.n_items > 0)
+                e = xm::plan_make(L, (const xm::JobDev *)ctx->d_jobs, (int)n_jobs, P.n_items, tile_off, n_normal,
+                                  n_heavy, ctx->d_plans, ctx->counters + 7, st);
+            if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev[2], st, ev_flags);
+            if (e == cudaSuccess && P.n_items > 0)
+                e = xm::run_pairs(L, (const xm::JobDev *)ctx->d_jobs, ctx->d_plans, n_normal, n_heavy, out, st);
+            if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev[3], st, ev_flags);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(ctx->h_counters, ctx->counters, 16 * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, st);
+            return e;
+        };
+        if (use_graph) {
+            // captured into a graph; the context's executable graph is updated
+            // in place when the launch sequence keeps its shape, else rebuilt
+            XM_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            cudaError_t e = enqueue(cudaEventRecordExternal);
+            cudaGraph_t g = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(st, &g);
+            if (e == cudaSuccess) e = e2;
+            if (e == cudaSuccess && ctx->graph_exec) {
+                cudaGraphExecUpdateResultInfo info;
+                if (cudaGraphExecUpdate(ctx->graph_exec, g, &info) != cudaSuccess) {
+                    cudaGetLastError();   // an update that does not fit is not an error
+                    cudaGraphExecDestroy(ctx->graph_exec);
+                    ctx->graph_exec = nullptr;
+                }
+            }
+            if (e == cudaSuccess && !ctx->graph_exec) e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e == cudaSuccess) e = cudaGraphLaunch(ctx->graph_exec, st);
+            XM_CUDA(ctx, e);
+            ctx->graph_launches++;
+        } else {
+            XM_CUDA(ctx, enqueue(cudaEventRecordDefault));
+        }
         XM_CUDA(ctx, cudaStreamSynchronize(st));
         cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
         if (retries == 0) cudaEventElapsedTime(&plan_ms, ctx->ev[14], ctx->ev[2]);

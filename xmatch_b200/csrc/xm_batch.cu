@@ -5,9 +5,13 @@
 // pulls jobs under a mutex (NextPreferredJob, JobManager.cpp:16-41;
 // Worker::operator(), Worker.cu:430-485), launching one kernel per zone pair
 // for each.  Here all jobs' tiles form one work list that the persistent
-// pair kernel drains with an atomic counter; matches carry their job index
-// and are grouped by job with a counting sort afterwards.  The launch
-// sequence is captured once in a CUDA graph and replayed.
+// pair kernel drains with an atomic counter (heavy pieces first, then tiles
+// in chunks); matches carry their job index and are grouped by job with a
+// counting sort afterwards.  After the host has read the tile totals, the
+// launch sequence (counters cleared, tile plans, pair kernel, counters read
+// back) runs as a CUDA graph held by the context: captured on every call and
+// applied to the executable graph by an in-place update, so a batch of
+// thousands of jobs is one graph launch (xm_run_jobs, xm_api.cu).
 #include <algorithm>
 #include <cstring>
 #include <vector>

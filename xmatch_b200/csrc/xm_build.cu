@@ -743,25 +743,7 @@ static xm_status build_lsd(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_s
     }
     seg->raq_bits = raq_bits;
     uint32_t launches = 0;
-    // storage
-    if (seg->cap < n || !seg->id) {
-        xm_dev_free(ctx, seg->id);
-        xm_dev_free(ctx, seg->radec);
-        xm_dev_free(ctx, seg->xyz);
-        xm_dev_free(ctx, seg->xyz64);
-        seg->id = nullptr; seg->radec = nullptr; seg->xyz = nullptr; seg->xyz64 = nullptr;
-        seg->cap = 0;
-        uint64_t c = std::max<uint64_t>(n, 1);
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->id, (c + 2) * sizeof(int64_t)));
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->radec, c * sizeof(double2)));
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz, c * sizeof(float4)));
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz64, (c + 2) * 3 * sizeof(double)));
-        seg->cap = c;
-    }
-    if (!seg->zone_off) {
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->zone_off, ((size_t)nz + 8) * 4));
-        XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0, ((size_t)nz + 8) * 4, st));
-    }
+    XM_TRY(xm_seg_storage(seg, n));
     const uint64_t nn = std::max<uint64_t>(n, 1);
     const uint32_t n_tiles = (uint32_t)((nn + kTile - 1) / kTile);
     // scratch: keys x2, vals x2, tile counts and offsets, scan scratch, histograms
@@ -769,8 +751,8 @@ static xm_status build_lsd(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_s
     const size_t cb = (((size_t)n_tiles * 256 * 4 + 4 + 255) & ~(size_t)255);
     const size_t sb = ((xm_scan_tmp_bytes((size_t)n_tiles * 256) + 255) & ~(size_t)255);
     const size_t hb = kMaxPasses * 256 * 4 + 64;
-    XM_TRY(ensure(ctx, &seg->tmp, &seg->tmp_bytes, 2 * kb + 2 * vb + 2 * cb + sb + hb));
-    char *w = (char *)seg->tmp;
+    XM_TRY(ensure(ctx, &ctx->build_tmp, &ctx->build_tmp_bytes, 2 * kb + 2 * vb + 2 * cb + sb + hb));
+    char *w = (char *)ctx->build_tmp;
     unsigned long long *k0 = (unsigned long long *)w; w += kb;
     unsigned long long *k1 = (unsigned long long *)w; w += kb;
     uint32_t *v0 = (uint32_t *)w; w += vb;
@@ -861,27 +843,29 @@ static xm_status build_lsd(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_s
     return XM_OK;
 }
 
-static xm_status seg_storage(xm_segment *seg, uint64_t n)
+// The segment's arrays live in one allocation (fewer, equal-sized blocks keep
+// the context's memory pool from fragmenting when segments come and go):
+// zone_off, id, radec, xyz, xyz64, each 256-byte aligned.
+xm_status xm_seg_storage(xm_segment *seg, uint64_t n)
 {
     xm_ctx *ctx = seg->ctx;
-    if (seg->cap < n || !seg->id) {
-        xm_dev_free(ctx, seg->id);
-        xm_dev_free(ctx, seg->radec);
-        xm_dev_free(ctx, seg->xyz);
-        xm_dev_free(ctx, seg->xyz64);
-        seg->id = nullptr; seg->radec = nullptr; seg->xyz = nullptr; seg->xyz64 = nullptr;
-        seg->cap = 0;
-        uint64_t c = std::max<uint64_t>(n, 1);
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->id, (c + 2) * sizeof(int64_t)));
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->radec, c * sizeof(double2)));
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz, c * sizeof(float4)));
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->xyz64, (c + 2) * 3 * sizeof(double)));
-        seg->cap = c;
-    }
-    if (!seg->zone_off) {
-        XM_TRY(xm_dev_alloc(ctx, (void **)&seg->zone_off, ((size_t)seg->n_zones + 8) * 4));
-        XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0, ((size_t)seg->n_zones + 8) * 4, ctx->stream));
-    }
+    if (seg->store && seg->cap >= n) return XM_OK;
+    const uint64_t c = std::max<uint64_t>(n, 1);
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t bz = al(((size_t)seg->n_zones + 8) * 4), bi = al((c + 2) * 8), br = al(c * 16), bx = al(c * 16),
+                 b6 = al((c + 2) * 24);
+    xm_dev_free(ctx, seg->store);
+    seg->store = nullptr;
+    seg->cap = 0;
+    XM_TRY(xm_dev_alloc(ctx, &seg->store, bz + bi + br + bx + b6));
+    char *w = (char *)seg->store;
+    seg->zone_off = (uint32_t *)w; w += bz;
+    seg->id = (int64_t *)w; w += bi;
+    seg->radec = (double2 *)w; w += br;
+    seg->xyz = (float4 *)w; w += bx;
+    seg->xyz64 = (double *)w;
+    seg->cap = c;
+    XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0, bz, ctx->stream));
     return XM_OK;
 }
 
@@ -896,7 +880,7 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     int raq_bits, passes;
     xm_raq_layout(nz, &raq_bits, &passes);
     seg->raq_bits = raq_bits;
-    XM_TRY(seg_storage(seg, n));
+    XM_TRY(xm_seg_storage(seg, n));
     const uint64_t nn = std::max<uint64_t>(n, 1);
     // buckets of 2^shift zones, at least 4 per SM
     int shift = kBucketMaxShift;
@@ -909,8 +893,8 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     const size_t bb = (((size_t)n_buckets + 1) * 4 + 255) & ~(size_t)255;
     const size_t sb = (xm_scan_tmp_bytes((size_t)nz) + 255) & ~(size_t)255;
     const size_t mb = 256;
-    XM_TRY(ensure(ctx, &seg->tmp, &seg->tmp_bytes, 2 * rb + 2 * zb + bb + sb + mb));
-    char *w = (char *)seg->tmp;
+    XM_TRY(ensure(ctx, &ctx->build_tmp, &ctx->build_tmp_bytes, 2 * rb + 2 * zb + bb + sb + mb));
+    char *w = (char *)ctx->build_tmp;
     ZRec *recs_b = (ZRec *)w; w += rb;
     ZRec *recs_z = (ZRec *)w; w += rb;
     uint32_t *cnt = (uint32_t *)w; w += zb;

@@ -5,14 +5,33 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <map>
 #include <unordered_map>
 #include <vector>
 
 #include "../../include/xmatch.h"
 
+// RA half-widths of one zone range for one (radius, zone height).
+struct xm_alpha_key {
+    uint64_t sr, zh;         // bit patterns of the doubles
+    int32_t z0, z1;          // zones [z0, z1]
+    bool operator<(const xm_alpha_key &o) const
+    {
+        if (sr != o.sr) return sr < o.sr;
+        if (zh != o.zh) return zh < o.zh;
+        if (z0 != o.z0) return z0 < o.z0;
+        return z1 < o.z1;
+    }
+};
 struct xm_alpha_entry {
-    double *dev = nullptr;   // [n_zones] RA half-width per zone (radians, 180 = no cut)
-    int32_t n_zones = 0;
+    double *dev = nullptr;   // [z1 - z0 + 1] radians (180 = no cut)
+    size_t bytes = 0;
+};
+// One request of xm_get_alpha_ranges; dev is filled in.
+struct xm_alpha_req {
+    double sr_deg, zh_deg;
+    int32_t z0, z1;
+    const double *dev;
 };
 
 // Device result of the last match call (library-owned, grown on demand).
@@ -41,7 +60,8 @@ struct xm_ctx {
     // counters: [0] matches, [1] tiles claimed, [2..] statistics
     unsigned long long *counters = nullptr;   // device, 16 entries
     unsigned long long *h_counters = nullptr; // pinned host mirror
-    std::unordered_map<uint64_t, xm_alpha_entry> alpha_cache;  // key: hash(sr, zh)
+    std::map<xm_alpha_key, xm_alpha_entry> alpha_cache;
+    size_t alpha_bytes = 0;
     xm_result_buf res;
     // job table and tile pre-pass buffers
     void *d_jobs = nullptr;
@@ -51,6 +71,12 @@ struct xm_ctx {
     void *d_plans = nullptr;     // tile plans
     size_t d_plans_bytes = 0;
     uint32_t *h_tiles = nullptr; // pinned: tile totals read back after the count pass
+    void *build_tmp = nullptr;   // zone-build scratch, shared by the context's builds
+    void *stage = nullptr;       // host records copied here by xm_segment_build
+    size_t stage_bytes = 0;
+    size_t build_tmp_bytes = 0;
+    cudaGraphExec_t graph_exec = nullptr;   // the pair-kernel launch sequence (see xm_run_jobs)
+    uint64_t graph_launches = 0;
 };
 
 struct xm_segment {
@@ -64,16 +90,16 @@ struct xm_segment {
     int32_t z_lo = 0, z_hi = -1;   // first / last zone holding an object
     int raq_bits = 32;             // leading bits of the quantised ra kept in xyz.w
     uint32_t dropped_host = 0;
+    void *store = nullptr;         // one allocation holding the arrays below
     uint32_t *zone_off = nullptr;  // [n_zones + 8]; [n_zones + 1] = dropped count; the rest
                                    // pads 16-byte bulk copies of zone-offset slices
     int64_t *id = nullptr;
     double2 *radec = nullptr;      // radians
     float4 *xyz = nullptr;         // FP32 unit vector; w = quantised-ra bits
     double *xyz64 = nullptr;       // FP64 unit vector (x, y, z) per object, 2 spare objects
-    // scratch kept for rebuilds
-    void *tmp = nullptr;           // radix-sort scratch
-    size_t tmp_bytes = 0;
 };
+// Allocates (or keeps, when large enough) the segment's arrays for n objects.
+xm_status xm_seg_storage(xm_segment *seg, uint64_t n);
 
 // ---- error plumbing ----
 #define XM_CUDA(ctx, call)                                                       \
@@ -94,8 +120,9 @@ struct xm_segment {
 // ---- internal entry points shared between translation units ----
 xm_status xm_dev_alloc(xm_ctx *ctx, void **p, size_t bytes);
 void xm_dev_free(xm_ctx *ctx, void *p);
-xm_status xm_get_alpha(xm_ctx *ctx, double sr_deg, double zh_deg, int32_t n_zones,
-                       const double **dev_alpha);
+// Device tables of RA half-widths for each request's zone range (cached).
+xm_status xm_get_alpha_ranges(xm_ctx *ctx, xm_alpha_req *req, size_t n);
+void alpha_cache_clear(xm_ctx *ctx);
 void xm_host_alpha_table(double sr_deg, double zh_deg, int32_t n_zones, double *out);
 
 // exclusive scan of n uint32 values (out[n] = total); tmp from xm_scan_tmp_bytes

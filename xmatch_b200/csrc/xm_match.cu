@@ -653,7 +653,7 @@ __device__ __forceinline__ uint32_t tile_pieces(const JobDev &J, uint32_t len, i
     const uint32_t nseg = (uint32_t)(band_hi - band_lo + 1);
     const uint32_t b_len = J.b_zoff[band_hi + 1] - J.b_zoff[band_lo];
     *piece = b_len;
-    const bool full_ring = J.alpha[zf] >= 3.0 || J.alpha[zl] >= 3.0;
+    const bool full_ring = J.alpha[zf - J.alpha_z0] >= 3.0 || J.alpha[zl - J.alpha_z0] >= 3.0;
     if (!full_ring || (int)nseg > kMaxBand || (uint64_t)len * b_len <= kHeavyPairs) return 1;
     uint32_t pc = max(32u, kHeavyPairs / max(len, 1u));
     pc = min(pc, cap_b);
@@ -729,8 +729,8 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
         uint32_t mode = PLAN_GLOBAL;
         if ((int)nseg <= kMaxBand && P.b_len <= cap_b) {
             mode = PLAN_WHOLE;
-        } else if (zf == zl && (int)nseg <= kMaxPlanSeg && J.alpha[zf] < 3.0) {
-            const double alpha = J.alpha[zf];
+        } else if (zf == zl && (int)nseg <= kMaxPlanSeg && J.alpha[zf - J.alpha_z0] < 3.0) {
+            const double alpha = J.alpha[zf - J.alpha_z0];
             // A is ordered by raq: every tile object's ra is within one raq step q of
             // [ra_first, ra_last]; widen by 2q
             const double q2 = 2.0 * ldexp(XM_TWO_PI, J.raq_shift - 32);
@@ -998,12 +998,12 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 a.dec = ra.y;
                 a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
                 a.zone = a_zone(J.a_zoff, S.zf, S.zl, S.a_start + t);
-                if (a.zone < 0 || a.zone >= K.n_zones) {
+                if (a.zone < J.alpha_z0 || a.zone > J.z_hi) {   // outside the job's zones and its alpha table
                     atomicExch(&out.counters[7], 1ull);
                     a.zone = 0;
                     a.alpha = -1.0;   // empty windows, no candidates
                 } else {
-                    a.alpha = __ldg(&J.alpha[a.zone]);
+                    a.alpha = __ldg(&J.alpha[a.zone - J.alpha_z0]);
                 }
                 a.full_ring = a.alpha >= 3.0;
                 a.id = S.a_id[S.id_skew + t];
@@ -1039,12 +1039,12 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 ra_a = rd.x;
                 dec_a = rd.y;
                 za = a_zone(J.a_zoff, S.zf, S.zl, S.a_start + t);
-                if (za < 0 || za >= K.n_zones) {
+                if (za < J.alpha_z0 || za > J.z_hi) {
                     atomicExch(&out.counters[7], 1ull);
                     za = 0;
                     alpha = -1.0;
                 } else {
-                    alpha = __ldg(&J.alpha[za]);
+                    alpha = __ldg(&J.alpha[za - J.alpha_z0]);
                 }
                 const Win wn = make_win(ra_a, alpha, K.raq_shift);
                 n = lane_ranges(V, K, wn, alpha >= 3.0, za, L.r[lane], nr);

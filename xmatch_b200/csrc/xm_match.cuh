@@ -17,7 +17,7 @@ struct JobDev {
     const float4 *b_xyz;
     const double *b_xyz64;
     const uint32_t *b_zoff;    // [n_zones + 1]
-    const double *alpha;       // [n_zones] RA half-width of A's zones
+    const double *alpha;       // RA half-width of A's zone z at alpha[z - alpha_z0], z in [z_lo, z_hi]
     double sr_rad, sr_dist2;
     float thr_hi, thr_lo;
     int n_zones, nz;
@@ -25,7 +25,7 @@ struct JobDev {
     uint32_t nA;               // objects of A
     uint32_t item_begin;       // first global work item of this job
     int raq_shift;             // xyz.w holds raq32(ra) >> raq_shift
-    int pad;
+    int alpha_z0;
 };
 
 struct MatchOut {
