@@ -163,6 +163,45 @@ xm_status xm_match_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint3
 xm_status xm_autotune_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags,
                             xm_tuning *best, float *best_ms, float *fixed_ms);
 
+/* ---- serving: a resident catalog answering a stream of query catalogs ----
+ * Replaces the reference's run-to-completion driver (_main,
+ * BoostXmatch.cpp:247-330, which loads, sorts and matches one catalog pair
+ * per process) with a request loop: the catalog segment stays in HBM, query
+ * catalogs are queued by xm_serve_submit, admitted while their estimated
+ * device memory fits the budget, zone-built on a second stream while the
+ * previous batch is matched, and matched together in one persistent launch
+ * (the xm_match_batch path, query = A side, catalog = B side).  Results are
+ * the same as xm_match of the query segment against the catalog. */
+typedef struct xm_server xm_server;
+typedef struct xm_serve_cfg {
+    uint64_t mem_budget;   /* device bytes for queries in flight; 0 = half the free memory at open */
+    uint32_t max_batch;    /* queries per batch at most; 0 = 1024 */
+    uint32_t flags;        /* match flags of every query (XM_FILTER32, XM_NO_DIST, ...) */
+} xm_serve_cfg;
+typedef struct xm_serve_info {
+    double t_submit_ms;    /* host clock (ms since the server opened) at submit */
+    double t_admit_ms;     /* admitted (memory reserved, build started) */
+    double t_done_ms;      /* results ready on the host */
+    uint32_t batch;        /* batch number that matched it */
+    uint32_t batch_size;   /* queries in that batch */
+    uint64_t count;        /* matches */
+} xm_serve_info;
+/* Opens a server on a catalog built on ctx's device; the catalog must outlive
+ * the server.  The server owns a second context (stream) for query builds and
+ * two host threads; ctx must not be used by the caller until xm_serve_close. */
+xm_status xm_serve_open(xm_ctx *ctx, const xm_segment *catalog, const xm_serve_cfg *cfg, xm_server **out);
+/* Queues a query catalog (host records, copied) with its radius; returns at
+ * once with a ticket.  XM_ERR_TOO_LARGE if the query alone exceeds the budget. */
+xm_status xm_serve_submit(xm_server *srv, const xm_obj *objs, uint64_t n, double sr_deg, uint64_t *ticket);
+/* Result of a ticket.  wait != 0 blocks until it is ready; otherwise XM_ERR_BUSY
+ * while it is pending.  With out NULL or without buffers only out->count and
+ * info are filled and the result is kept; XM_ERR_CAPACITY (out->count set,
+ * result kept) when the buffers are too small; otherwise the matches are
+ * copied and the ticket is released.  A failed query returns its error once. */
+xm_status xm_serve_poll(xm_server *srv, uint64_t ticket, int wait, xm_pairs *out, xm_serve_info *info);
+/* Finishes every queued query, stops the threads and frees the server. */
+xm_status xm_serve_close(xm_server *srv);
+
 /* ---- formats (Segment::Load, Segment.cpp:14-22; output, Worker.cu:407-420) ---- */
 /* Number of 24-byte records in a .idradec file. */
 xm_status xm_idradec_count(const char *path, uint64_t *n);

@@ -133,6 +133,53 @@ class DeviceSegment:
             pass
 
 
+class Server:
+    """A resident catalog answering query catalogs (xm_serve_*): submit() queues a
+    query and returns a ticket, poll() returns (pairs, dist, info) once it is done.
+    The context is the server's until close()."""
+
+    def __init__(self, ctx, catalog, mem_budget=0, max_batch=0, flags=XM_FILTER32):
+        self.ctx = ctx
+        self.catalog = catalog
+        self.with_dist = (flags & XM_NO_DIST) == 0
+        cfg = _capi.XmServeCfg(mem_budget, max_batch, flags)
+        h = ctypes.c_void_p()
+        _check(_lib.xm_serve_open(ctx._h, catalog.handle, ctypes.byref(cfg), ctypes.byref(h)), ctx._h)
+        self._h = h
+
+    def submit(self, objs, sr_deg):
+        objs = as_objs(objs)
+        t = ctypes.c_uint64()
+        _check(_lib.xm_serve_submit(self._h, _ptr(objs), len(objs), sr_deg, ctypes.byref(t)), self.ctx._h)
+        return t.value
+
+    def poll(self, ticket, wait=True):
+        """(pairs, dist, info dict), or None if not ready and wait is False."""
+        info = _capi.XmServeInfo()
+        p = XmPairs(None, None, 0, 0)
+        rc = _lib.xm_serve_poll(self._h, ticket, 1 if wait else 0, ctypes.byref(p), ctypes.byref(info))
+        if rc == _capi.XM_ERR_BUSY:
+            return None
+        _check(rc, self.ctx._h)
+        n = p.count
+        pairs = np.empty((max(n, 1), 2), np.int64)
+        dist = np.empty(max(n, 1), np.float64) if self.with_dist else None
+        p = XmPairs(_ptr(pairs), _ptr(dist), n, 0)
+        _check(_lib.xm_serve_poll(self._h, ticket, 1, ctypes.byref(p), ctypes.byref(info)), self.ctx._h)
+        return pairs[:n], (dist[:n] if self.with_dist else None), info.as_dict()
+
+    def close(self):
+        if self._h:
+            _check(_lib.xm_serve_close(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class Context:
     """One GPU (replaces CudaManager/CudaContext)."""
 

@@ -59,6 +59,18 @@ class XmTuning(ctypes.Structure):
                 ("zones", ctypes.c_uint32)]
 
 
+class XmServeCfg(ctypes.Structure):
+    _fields_ = [("mem_budget", ctypes.c_uint64), ("max_batch", ctypes.c_uint32), ("flags", ctypes.c_uint32)]
+
+
+class XmServeInfo(ctypes.Structure):
+    _fields_ = [("t_submit_ms", ctypes.c_double), ("t_admit_ms", ctypes.c_double), ("t_done_ms", ctypes.c_double),
+                ("batch", ctypes.c_uint32), ("batch_size", ctypes.c_uint32), ("count", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class XmJob(ctypes.Structure):
     _fields_ = [("A", ctypes.c_void_p), ("B", ctypes.c_void_p), ("sr_deg", ctypes.c_double)]
 
@@ -101,6 +113,10 @@ SIGNATURES = {
     "xm_segment_build_noalloc": (ctypes.c_int, [ctypes.c_int, P, P, U64, D, P, P, P, P, U64,
                                                 ctypes.POINTER(U64)]),
     "xm_alpha_table": (ctypes.c_int, [D, D, P, I32]),
+    "xm_serve_open": (ctypes.c_int, [P, P, ctypes.POINTER(XmServeCfg), PP]),
+    "xm_serve_submit": (ctypes.c_int, [P, P, U64, D, ctypes.POINTER(U64)]),
+    "xm_serve_poll": (ctypes.c_int, [P, U64, ctypes.c_int, ctypes.POINTER(XmPairs), ctypes.POINTER(XmServeInfo)]),
+    "xm_serve_close": (ctypes.c_int, [P]),
 }
 
 

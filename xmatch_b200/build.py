@@ -23,7 +23,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-co
                   "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]
 CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall", "-I" + os.path.join(HERE, "..", "include")]
 
-CU_SOURCES = ["xm_scan.cu", "xm_build.cu", "xm_match.cu", "xm_batch.cu", "xm_api.cu"]
+CU_SOURCES = ["xm_scan.cu", "xm_build.cu", "xm_match.cu", "xm_batch.cu", "xm_api.cu", "xm_serve.cu"]
 CXX_SOURCES = ["xm_io.cpp"]
 
 

@@ -504,8 +504,8 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
     std::vector<uint32_t> ajob;
     for (uint32_t j = 0; j < n_jobs; ++j) {
         const xm_segment *A = jobs[j].A, *B = jobs[j].B;
-        if (!A || !B || A->ctx != ctx || B->ctx != ctx) {
-            ctx->last_error = "job " + std::to_string(j) + ": missing segment or segment of another context";
+        if (!A || !B || A->ctx->device != ctx->device || B->ctx->device != ctx->device) {
+            ctx->last_error = "job " + std::to_string(j) + ": missing segment or segment on another device";
             return XM_ERR_INVALID;
         }
         if (A->zh_deg != B->zh_deg || A->n_zones != B->n_zones) {

@@ -19,9 +19,6 @@
 #include "xm_internal.h"
 #include "xm_match.cuh"
 
-xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags, const xm_tuning *tuning,
-                      bool want_job, xm_stats *stats, float *kernel_ms);
-
 namespace {
 
 constexpr int kHistSmem = 8192;
@@ -78,7 +75,7 @@ __global__ void job_scatter(const uint32_t *__restrict__ job, const longlong2 *_
 }  // namespace
 
 // Groups ctx->res by job into pairs_g/dist_g and fills res.job_off.
-static xm_status group_by_job(xm_ctx *ctx, uint32_t n_jobs, uint32_t *n_launch)
+xm_status xm_group_by_job(xm_ctx *ctx, uint32_t n_jobs, uint32_t *n_launch)
 {
     xm_result_buf &r = ctx->res;
     cudaStream_t st = ctx->stream;
@@ -135,7 +132,7 @@ extern "C" xm_status xm_match_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_
     XM_TRY(xm_run_jobs(ctx, jobs, n_jobs, flags, tuning, n_jobs > 1, stats, nullptr));
     uint32_t launches = 0;
     if (n_jobs > 1) {
-        XM_TRY(group_by_job(ctx, n_jobs, &launches));
+        XM_TRY(xm_group_by_job(ctx, n_jobs, &launches));
     } else {
         ctx->res.job_off = {0ull, (uint64_t)ctx->res.count};
         ctx->res.grouped = false;

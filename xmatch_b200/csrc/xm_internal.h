@@ -120,6 +120,11 @@ xm_status xm_seg_storage(xm_segment *seg, uint64_t n);
 // ---- internal entry points shared between translation units ----
 xm_status xm_dev_alloc(xm_ctx *ctx, void **p, size_t bytes);
 void xm_dev_free(xm_ctx *ctx, void *p);
+// Runs the pair kernel over the jobs; ctx->res holds the (ungrouped) matches.
+xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags, const xm_tuning *tuning,
+                      bool want_job, xm_stats *stats, float *kernel_ms);
+// Groups ctx->res by job (res.pairs_g, res.dist_g, res.job_off).
+xm_status xm_group_by_job(xm_ctx *ctx, uint32_t n_jobs, uint32_t *n_launch);
 // Device tables of RA half-widths for each request's zone range (cached).
 xm_status xm_get_alpha_ranges(xm_ctx *ctx, xm_alpha_req *req, size_t n);
 void alpha_cache_clear(xm_ctx *ctx);
