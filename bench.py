@@ -54,6 +54,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
+    ap.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
+                    help="c1: 50Mx50M crossmatch (the headline); c2: 4,096-job batch; c3: precision stress; "
+                         "c4: serving")
+    ap.add_argument("--c2-jobs", type=int, default=4096)
+    ap.add_argument("--c2-scale", type=float, default=1.0, help="scale of the c2 per-job sizes")
+    ap.add_argument("--c3-n", type=int, default=10_000_000)
+    ap.add_argument("--c3-planted", type=int, default=1_000_000)
+    ap.add_argument("--c4-catalog", type=int, default=500_000_000, help="resident catalog size")
+    ap.add_argument("--c4-queries", type=int, default=400)
+    ap.add_argument("--c4-rate", type=float, default=100.0, help="Poisson arrival rate (queries/s)")
+    ap.add_argument("--c4-alone", type=int, default=24, help="queries also timed alone (plain FP64 kernel)")
     return ap.parse_args()
 
 
@@ -405,10 +416,277 @@ def run_ours(args):
     return 0
 
 
+def emit(args, line):
+    s = json.dumps(line)
+    print(s, flush=True)
+    if args.out:
+        with open(args.out, "a") as f:
+            f.write(s + "\n")
+
+
+def event_ms(stream, fn, steps, warmup):
+    """Device time per call of fn() (CUDA events on the library's stream)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_c2(args):
+    """Config 2: thousands of uneven segment-pair jobs (LogNormal sizes, own
+    radius and zone height each) in one persistent launch; autotuned tuning vs
+    the fixed one, graph vs direct launches, FP32 filter vs plain FP64, and the
+    reference-style loop of one match per job."""
+    import torch
+    import xmatch_b200 as xm
+    from xmatch_b200 import synth
+    torch.cuda.set_device(0)
+    jobs = synth.config2_jobs(n_jobs=args.c2_jobs, scale=args.c2_scale)
+    ctx = xm.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", 0))
+    t0 = time.perf_counter()
+    segs = [(ctx.build(A, r * ARCSEC), ctx.build(B, r * ARCSEC), r * ARCSEC) for A, B, r in jobs]
+    build_s = time.perf_counter() - t0
+    n_a = sum(len(A) for A, _, _ in jobs)
+    n_b = sum(len(B) for _, B, _ in jobs)
+    _, cnt, st = ctx.match_batch(segs, xm.XM_COUNT_CAND, fetch=False)
+    n_cand, n_match = st["n_cand"], sum(cnt)
+    tuning, tune_best_ms, tune_fixed_ms = ctx.autotune(segs)
+    fixed = (128, 16, 0, 16)
+    K, W = args.steps, max(args.warmup, 3)
+    ms = {
+        "autotuned": event_ms(stream, lambda: ctx.match_batch(segs, 0, tuning=tuning, fetch=False), K, W),
+        "fixed": event_ms(stream, lambda: ctx.match_batch(segs, 0, tuning=fixed, fetch=False), K, W),
+        "autotuned_no_graph": event_ms(stream, lambda: ctx.match_batch(segs, xm.XM_NO_GRAPH, tuning=tuning,
+                                                                        fetch=False), K, W),
+        "plain64": event_ms(stream, lambda: ctx.match_batch(segs, xm.XM_PLAIN64, tuning=tuning, fetch=False), K, W),
+        "loop_of_single_matches": event_ms(stream, lambda: [ctx.match(a, b, r, 0, fetch=False) for a, b, r in segs],
+                                           1, 1),
+    }
+    t0 = time.perf_counter()
+    res, _, _ = ctx.match_batch(segs, 0, tuning=tuning)
+    e2e_s = time.perf_counter() - t0
+    got = sum(len(p) for p, _ in res)
+    if got != n_match:
+        raise RuntimeError("batch returned %d matches, expected %d" % (got, n_match))
+    v = n_cand / (ms["autotuned"] * 1e-3)
+    emit(args, {
+        "metric": "config2 batch candidate pairs/s", "value": v, "unit": UNIT, "n_gpus": 1, "steps": K,
+        "warmup": W, "ms_per_step": ms["autotuned"], "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded config2 jobs; no survey data)",
+        "config": {"workload": "config2 %d jobs, LogNormal(20k, 1) sizes x %g, dec bands 0.5-5 deg, r = zh ~ U[0.5, 5]\""
+                   % (len(jobs), args.c2_scale), "objects_a": n_a, "objects_b": n_b},
+        "candidates": n_cand, "matches": n_match, "jobs_per_s": len(jobs) / (ms["autotuned"] * 1e-3),
+        "tuning": {"autotuned": list(tuning), "fixed": list(fixed), "autotune_best_ms": tune_best_ms,
+                   "autotune_fixed_ms": tune_fixed_ms},
+        "ms": ms, "speedup_vs_loop": ms["loop_of_single_matches"] / ms["autotuned"],
+        "speedup_vs_plain64": ms["plain64"] / ms["autotuned"],
+        "e2e": {"seconds": e2e_s, "what": "one xm_match_batch with results copied to host and split by job"},
+        "segment_build_s": build_s,
+    })
+    for a, b, _ in segs:
+        a.free()
+        b.free()
+    ctx.close()
+    return 0
+
+
+def run_c3(args):
+    """Config 3: precision stress, uniform catalogs plus planted pairs at
+    r (1 +- k 1e-9): every '-' pair must be found and no '+' pair, at r = 0.1"
+    and 60"; reports the fraction of tested pairs in the FP32 margin band."""
+    import torch
+    import xmatch_b200 as xm
+    from xmatch_b200 import synth
+    torch.cuda.set_device(0)
+    ctx = xm.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", 0))
+    out = {}
+    K, W = args.steps, max(args.warmup, 3)
+    for r_arcsec in (0.1, 60.0):
+        A, B, sign, kk = synth.config3(n=args.c3_n, n_planted=args.c3_planted, r_arcsec=r_arcsec)
+        res = kk * 1e-9 * np.radians(r_arcsec * ARCSEC) >= 1e-13   # offset above the FP64 spacing of coordinates
+        r = r_arcsec * ARCSEC
+        sa, sb = ctx.build(A, r), ctx.build(B, r)
+        p, _, st = ctx.match(sa, sb, r, xm.XM_COUNT_CAND)
+        n = args.c3_n
+        hit = np.zeros(len(sign), bool)
+        pl = (p[:, 0] >= n) & (p[:, 1] - 100_000_000_000 == p[:, 0])
+        hit[p[pl, 0] - n] = True
+        p64, _, st64 = ctx.match(sa, sb, r, xm.XM_PLAIN64)
+        same = len(p64) == len(p) and np.array_equal(p64[np.lexsort((p64[:, 1], p64[:, 0]))],
+                                                    p[np.lexsort((p[:, 1], p[:, 0]))])
+        t32 = event_ms(stream, lambda: ctx.match(sa, sb, r, 0, fetch=False), K, W)
+        t64 = event_ms(stream, lambda: ctx.match(sa, sb, r, xm.XM_PLAIN64, fetch=False), K, W)
+        out["r=%g\"" % r_arcsec] = {
+            "matches": len(p), "candidates": st["n_cand"], "tested": st["n_tested"],
+            "borderline": st["n_border"], "borderline_fraction": st["n_border"] / max(st["n_tested"], 1),
+            "fp64_decisions": st["n_exact"],
+            "planted_minus_found": int(np.sum(hit & (sign < 0))), "planted_minus": int(np.sum(sign < 0)),
+            "planted_plus_found": int(np.sum(hit & (sign > 0))), "planted_plus": int(np.sum(sign > 0)),
+            "planted_resolvable": int(np.sum(res)),
+            "planted_resolvable_wrong": int(np.sum(res & (hit != (sign < 0)))),
+            "filter32_equals_plain64": bool(same),
+            "ms_filter32": t32, "ms_plain64": t64, "speedup_filter32_vs_plain64": t64 / t32,
+        }
+        sa.free()
+        sb.free()
+    first = out["r=0.1\""]
+    emit(args, {
+        "metric": "config3 planted-pair exactness (r = 0.1\" and 60\")", "value": first["ms_filter32"],
+        "unit": "ms per match (r = 0.1\")", "n_gpus": 1, "steps": K, "warmup": W, "higher_is_better": False,
+        "dtype": "f64", "data": "synthetic (seeded config3; no survey data)",
+        "config": {"workload": "config3 %d uniform + %d planted pairs per side" % (args.c3_n, args.c3_planted)},
+        "results": out,
+    })
+    ctx.close()
+    return 0
+
+
+def cap_points(rng, n, ra0, dec0, radius_deg):
+    """n points uniform in the spherical cap of the given radius around (ra0, dec0)."""
+    ct = rng.uniform(np.cos(np.radians(radius_deg)), 1.0, n)
+    st = np.sqrt(1 - ct * ct)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    v = np.stack([ct, st * np.cos(ph), st * np.sin(ph)], axis=-1)   # around +x
+    a, d = np.radians(ra0), np.radians(dec0)
+    ca, sa, cd, sd = np.cos(a), np.sin(a), np.cos(d), np.sin(d)
+    # rotate +x to (a, d): R = Rz(a) Ry(-d)
+    x = cd * v[:, 0] - sd * v[:, 2]
+    z = sd * v[:, 0] + cd * v[:, 2]
+    y = v[:, 1]
+    X, Y = ca * x - sa * y, sa * x + ca * y
+    ra = np.degrees(np.arctan2(Y, X)) % 360.0
+    dec = np.degrees(np.arcsin(np.clip(z, -1, 1)))
+    return ra, dec
+
+
+def run_c4(args):
+    """Config 4: serving.  A resident catalog (config 1 mixture, generated on
+    the GPU), query catalogs arriving as a Poisson stream (n ~ LogUniform[100,
+    1M], patch diameter U[0.1, 10] deg, r ~ U[0.5, 10]\"); p50/p99 latency from
+    submit to results on the host, matches/s; a sample of the queries is then
+    timed alone with the plain FP64 kernel."""
+    import threading
+    import torch
+    import xmatch_b200 as xm
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    N = args.c4_catalog
+    zh = 1.0 * ARCSEC
+    g = torch.Generator(device=dev)
+    g.manual_seed(1004)
+    nu = int(0.8 * N)
+    ra = torch.rand(N, dtype=torch.float64, device=dev, generator=g) * 360.0
+    dec = torch.empty(N, dtype=torch.float64, device=dev)
+    dec[:nu] = torch.rad2deg(torch.asin(torch.rand(nu, dtype=torch.float64, device=dev, generator=g) * 2 - 1))
+    hr = np.random.default_rng(1004)
+    cra = torch.from_numpy(hr.uniform(0, 360, 500)).to(dev)
+    cdec = torch.from_numpy(np.degrees(np.arcsin(hr.uniform(-1, 1, 500)))).to(dev)
+    which = torch.randint(0, 500, (N - nu,), device=dev, generator=g)
+    cd = cdec[which]
+    dec[nu:] = (cd + 0.1 * torch.randn(N - nu, dtype=torch.float64, device=dev, generator=g)).clamp(-90.0, 90.0)
+    ra[nu:] = torch.remainder(cra[which] + 0.1 * torch.randn(N - nu, dtype=torch.float64, device=dev, generator=g)
+                              / torch.cos(torch.deg2rad(cd)).clamp_min(1e-3), 360.0)
+    rec = torch.stack([torch.arange(N, dtype=torch.int64, device=dev), ra.view(torch.int64), dec.view(torch.int64)],
+                      dim=1).contiguous()
+    del ra, dec, which, cd
+    ctx = xm.Context(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cat = ctx.build_device(rec.data_ptr(), N, zh, 0)
+    cat_build_s = time.perf_counter() - t0
+    del rec
+    torch.cuda.empty_cache()
+    # query stream, generated before the clock starts
+    qr = np.random.default_rng(2004)
+    queries = []
+    for k in range(args.c4_queries):
+        n = int(np.exp(qr.uniform(np.log(100), np.log(1_000_000))))
+        diam = qr.uniform(0.1, 10.0)
+        c_ra, c_dec = qr.uniform(0, 360), np.degrees(np.arcsin(qr.uniform(-1, 1)))
+        ra_q, dec_q = cap_points(qr, n, c_ra, c_dec, diam / 2)
+        q = np.empty(n, xm.OBJ_DTYPE)
+        q["id"], q["ra"], q["dec"] = np.arange(n) + 10_000_000_000 * (k + 1), ra_q, dec_q
+        queries.append((q, qr.uniform(0.5, 10.0) * ARCSEC))
+    arrivals = np.cumsum(qr.exponential(1.0 / args.c4_rate, len(queries)))
+    srv = xm.Server(ctx, cat)
+    tickets = [None] * len(queries)
+    ready = threading.Event()
+
+    def submitter():
+        start = time.perf_counter()
+        for k, (q, r) in enumerate(queries):
+            d = start + arrivals[k] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[k] = srv.submit(q, r)
+            if k == 0:
+                ready.set()
+    th = threading.Thread(target=submitter)
+    th.start()
+    infos, matches = [], 0
+    for k in range(len(queries)):
+        while tickets[k] is None:
+            time.sleep(0.0005)
+        p, d, info = srv.poll(tickets[k])
+        infos.append(info)
+        matches += len(p)
+    th.join()
+    srv.close()
+    lat = np.array([i["t_done_ms"] - i["t_submit_ms"] for i in infos])
+    span_s = (max(i["t_done_ms"] for i in infos) - min(i["t_submit_ms"] for i in infos)) * 1e-3
+    batches = np.array([i["batch_size"] for i in infos])
+    # a sample alone: build + plain FP64 match + results to host, one query at a time
+    alone64, alone32 = [], []
+    for k in range(min(args.c4_alone, len(queries))):
+        q, r = queries[k]
+        for flags, acc in ((xm.XM_PLAIN64, alone64), (0, alone32)):
+            t = time.perf_counter()
+            s = ctx.build(q, zh)
+            ctx.match(s, cat, r, flags)
+            s.free()
+            acc.append((time.perf_counter() - t) * 1e3)
+    m = min(args.c4_alone, len(queries))
+    emit(args, {
+        "metric": "config4 serving p99 latency", "value": float(np.percentile(lat, 99)), "unit": "ms",
+        "n_gpus": 1, "higher_is_better": False, "dtype": "f64",
+        "data": "synthetic (config1 mixture catalog generated on the GPU; seeded query stream)",
+        "config": {"workload": "config4 resident %d-object catalog, %d queries, Poisson %.0f/s, n ~ LogUniform[100, 1M], "
+                   "patch U[0.1, 10] deg, r ~ U[0.5, 10]\"" % (N, len(queries), args.c4_rate), "zh_arcsec": 1.0},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
+                       "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+        "queries_per_s": len(queries) / span_s, "matches_per_s": matches / span_s, "matches": matches,
+        "objects_per_s": sum(len(q) for q, _ in queries) / span_s,
+        "batch_size": {"mean": float(batches.mean()), "max": int(batches.max())},
+        "alone_first_%d_queries_ms" % m: {"plain64_mean": float(np.mean(alone64)),
+                                          "filter32_mean": float(np.mean(alone32)),
+                                          "served_latency_mean": float(np.mean(lat[:m]))},
+        "catalog_build_s": cat_build_s,
+    })
+    cat.free()
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "c2":
+        return run_c2(args)
+    if args.config == "c3":
+        return run_c3(args)
+    if args.config == "c4":
+        return run_c4(args)
     return run_ours(args)
 
 

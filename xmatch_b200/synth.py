@@ -120,7 +120,9 @@ def config1(n=50_000_000, seed=1001, frac_pert=0.7, sigma_arcsec=0.3, edges=True
 
 def planted(rng, n_pairs, r_deg, kmax=100, rel=1e-9):
     """Pairs at separation r (1 +- k rel), k uniform in 1..kmax, random position angle.
-    Returns (A_ra, A_dec, B_ra, B_dec, sign) with sign +1 for r(1 + k rel) (outside)."""
+    Returns (A_ra, A_dec, B_ra, B_dec, sign, k) with sign +1 for r(1 + k rel) (outside).
+    The offset k rel r is only meaningful where it is well above the FP64 spacing
+    of the stored coordinates (about 1e-15 rad for degrees up to 360)."""
     ra, dec = uniform_sphere(rng, n_pairs)
     k = rng.integers(1, kmax + 1, n_pairs)
     sign = np.where(rng.random(n_pairs) < 0.5, 1.0, -1.0)
@@ -134,20 +136,21 @@ def planted(rng, n_pairs, r_deg, kmax=100, rel=1e-9):
     t = np.cos(pa)[:, None] * e_ra + np.sin(pa)[:, None] * e_de
     q = np.cos(sep)[:, None] * p + np.sin(sep)[:, None] * t
     bra, bdec = _radec(q)
-    return ra, dec, bra, bdec, sign
+    return ra, dec, bra, bdec, sign, k
 
 
 def config3(n=10_000_000, n_planted=1_000_000, r_arcsec=0.1, seed=1003):
-    """Precision stress: n uniform per side plus n_planted pairs at r(1 +- k 1e-9)."""
+    """Precision stress: n uniform per side plus n_planted pairs at r(1 +- k 1e-9).
+    Returns (A, B, sign, k); planted pair i is (A id n + i, B id 1e11 + n + i)."""
     rng = np.random.default_rng(seed)
     ra, dec = uniform_sphere(rng, n)
-    pra, pdec, qra, qdec, sign = planted(rng, n_planted, r_arcsec * ARCSEC)
+    pra, pdec, qra, qdec, sign, k = planted(rng, n_planted, r_arcsec * ARCSEC)
     A = make_objs(np.arange(n + n_planted, dtype=np.int64), np.concatenate([ra, pra]),
                   np.concatenate([dec, pdec]))
     rb, db = uniform_sphere(rng, n)
     B = make_objs(np.arange(n + n_planted, dtype=np.int64) + 100_000_000_000,
                   np.concatenate([rb, qra]), np.concatenate([db, qdec]))
-    return A, B, sign
+    return A, B, sign, k
 
 
 def config2_jobs(n_jobs=4096, seed=1002, median=20_000, sigma=1.0, lo=1_000, hi=2_000_000, scale=1.0):
