@@ -545,7 +545,10 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
             areq.push_back({p.sr_deg, A->zh_deg, A->z_lo, A->z_hi, nullptr});
             ajob.push_back(j);
         }
-        guess += 2 * std::max(A->n, B->n);   // Worker.cu:296-297 default
+        // first output size: 2 min(nA, nB) per job (Worker.cu:296-297 uses the max,
+        // which for a small query against a large catalog would reserve the
+        // catalog's size); an overflow reruns at the exact count
+        guess += 2 * std::min(A->n, B->n);
         if (items >= 0xFFFFFF00ull) {
             ctx->last_error = "too many work items in one launch";
             return XM_ERR_INVALID;
