@@ -63,10 +63,11 @@ extern "C" {
 // radec_*: [2 n] radians (ra, dec) grouped by zone; zbeg/zend: [n_zones].
 // Writes up to cap (iA, iB) pairs of segment-local indices, returns the
 // number of matches the kernel counted (may exceed cap), or -1 on error.
+// ms_loop (optional): device time of the zone loop.
 long long ref_xmatch(const double *radec_a, long long na, const int *zbeg_a, const int *zend_a,
                      const double *radec_b, long long nb, const int *zbeg_b, const int *zend_b, int n_zones,
                      double sr_deg, double zh_deg, unsigned int *pairs, unsigned int cap, int *launches,
-                     int validate, long long *outside, int pad)
+                     int validate, long long *outside, int pad, float *ms_loop)
 {
     using namespace xmatch;
     dbl2 *da = nullptr, *db = nullptr;
@@ -101,7 +102,13 @@ long long ref_xmatch(const double *radec_a, long long na, const int *zbeg_a, con
         const double sr_rad = sr_deg / RAD2DEG;
         double sr_dist2 = 2.0 * sin(sr_rad / 2.0);
         sr_dist2 *= sr_dist2;
-        // Worker.cu:330-366
+        // Worker.cu:330-366; timed with events around the whole zone loop (launch gaps included)
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        if (ms_loop) {
+            cudaEventCreate(&ev0);
+            cudaEventCreate(&ev1);
+            cudaEventRecord(ev0);
+        }
         for (int zid1 = 0; zid1 < n_zones; zid1++) {
             const int i1s = zbeg_a[zid1], i1e = zend_a[zid1], n1 = i1e - i1s;
             if (n1 < 1) continue;
@@ -143,8 +150,14 @@ long long ref_xmatch(const double *radec_a, long long na, const int *zbeg_a, con
             }
             if (failed) break;
         }
+        if (ms_loop) cudaEventRecord(ev1);
         if (failed) break;
         if (cudaDeviceSynchronize() != cudaSuccess) break;
+        if (ms_loop) {
+            cudaEventElapsedTime(ms_loop, ev0, ev1);
+            cudaEventDestroy(ev0);
+            cudaEventDestroy(ev1);
+        }
         if (validate) {
             result = (long long)kept;
             if (outside) *outside = out_n;

@@ -26,7 +26,8 @@ def lib():
         L.ref_xmatch.restype = ctypes.c_longlong
         L.ref_xmatch.argtypes = [P, ctypes.c_longlong, P, P, P, ctypes.c_longlong, P, P, ctypes.c_int,
                                  ctypes.c_double, ctypes.c_double, P, ctypes.c_uint, ctypes.POINTER(ctypes.c_int),
-                                 ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+                                 ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_float)]
         _lib = L
     return _lib
 
@@ -71,7 +72,7 @@ def xmatch(A, B, sr_deg, zh_deg=None, validate=True, pad=True):
         n = L.ref_xmatch(ra.ctypes.data, len(ia), zba.ctypes.data, zea.ctypes.data, rb.ctypes.data, len(ib),
                          zbb.ctypes.data, zeb.ctypes.data, n_zones, sr_deg, zh_deg, out.ctypes.data, cap,
                          ctypes.byref(launches), 1 if (validate or pad) else 0, ctypes.byref(outside),
-                         1 if pad else 0)
+                         1 if pad else 0, None)
         if n < 0:
             if cap >= 1 << 30:
                 raise RuntimeError("reference kernel harness failed")
@@ -83,3 +84,25 @@ def xmatch(A, B, sr_deg, zh_deg=None, validate=True, pad=True):
         p = out[:n].astype(np.int64)
         pairs = np.stack([A["id"][ia[p[:, 0]]], B["id"][ib[p[:, 1]]]], 1)
         return pairs, int(outside.value), launches.value
+
+
+def time_zone_loop(A, B, sr_deg, zh_deg=None):
+    """Device time of the reference's zone loop (Worker.cu:330-366) exactly as it
+    launches: its geometry, no per-launch synchronisation; inputs are copied to
+    the device before the clock starts.  Returns (seconds, launches, count)."""
+    if zh_deg is None:
+        zh_deg = sr_deg
+    n_zones = int(np.ceil(180 / zh_deg))
+    ia, ra, zba, zea = _zone_layout(A, zh_deg, n_zones)
+    ib, rb, zbb, zeb = _zone_layout(B, zh_deg, n_zones)
+    cap = max(1 << 16, 4 * (len(ia) + len(ib)))
+    out = np.empty((cap, 2), np.uint32)
+    launches = ctypes.c_int()
+    outside = ctypes.c_longlong()
+    ms = ctypes.c_float()
+    n = lib().ref_xmatch(ra.ctypes.data, len(ia), zba.ctypes.data, zea.ctypes.data, rb.ctypes.data, len(ib),
+                         zbb.ctypes.data, zeb.ctypes.data, n_zones, sr_deg, zh_deg, out.ctypes.data, cap,
+                         ctypes.byref(launches), 0, ctypes.byref(outside), 0, ctypes.byref(ms))
+    if n < 0:
+        raise RuntimeError("reference kernel harness failed")
+    return ms.value * 1e-3, launches.value, int(n)
