@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--e2e-dist", action="store_true",
                     help="e2e also returns distances (24-byte records instead of the reference's 16-byte pairs)")
+    ap.add_argument("--dec-band", type=float, nargs=2, default=None, metavar=("LO", "HI"),
+                    help="keep only sources with dec in [LO, HI) deg (same density, smaller case for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
@@ -254,7 +256,11 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     A, B = load_workload(args.n)
-    n = len(A)
+    if args.dec_band:
+        lo, hi = args.dec_band
+        A = A[(A["dec"] >= lo) & (A["dec"] < hi)]
+        B = B[(B["dec"] >= lo) & (B["dec"] < hi)]
+    n, nb = len(A), len(B)
     r = 1.0 * ARCSEC
     zh = 1.0 * ARCSEC
     flags = xm.XM_PLAIN64 if args.variant == "plain64" else xm.XM_FILTER32
@@ -266,14 +272,14 @@ def run_ours(args):
     dB = torch.from_numpy(B.view(np.uint8)).to(dev)
     torch.cuda.synchronize(dev)
     sa = ctx.build_device(dA.data_ptr(), n, zh, 0)
-    sb = ctx.build_device(dB.data_ptr(), n, zh, 1)
+    sb = ctx.build_device(dB.data_ptr(), nb, zh, 1)
     # candidate count (metric numerator) and match count, untimed
     _, _, st0 = ctx.match(sa, sb, r, flags | xm.XM_COUNT_CAND, fetch=False)
     n_cand, n_match = st0["n_cand"], st0["n_match"]
 
     def step(stats):
         sa.rebuild_device(dA.data_ptr(), n, stats)
-        sb.rebuild_device(dB.data_ptr(), n, stats)
+        sb.rebuild_device(dB.data_ptr(), nb, stats)
         ms_ = ctx.match(sa, sb, r, flags, fetch=False)[2]
         for k in ("ms_match", "ms_plan", "n_tested", "n_exact", "n_border", "n_launches"):
             setattr(stats, k, getattr(stats, k) + ms_[k])
@@ -309,11 +315,12 @@ def run_ours(args):
     }
     kept_a, kept_b = len(sa), len(sb)
     n_zones = int(np.ceil(180 / zh))
+    nc = (n + nb) // 2   # mean catalog size (the zb_* stages are per catalog)
     alg_bytes = {   # algorithmic bytes per launch (per catalog for the zb_* stages)
-        "zb_count": 24 * n,                        # records in
+        "zb_count": 24 * nc,                       # records in
         "zb_offsets": 16 * n_zones,                # counts in, offsets out, cursors
-        "zb_scatter": (24 + 32) * n,               # records in, 32-byte bucket records out
-        "zb_zone_sort": (32 + 64) * n,             # bucket records in; id, radec, xyz, xyz64 out
+        "zb_scatter": (24 + 32) * nc,              # records in, 32-byte bucket records out
+        "zb_zone_sort": (32 + 64) * nc,            # bucket records in; id, radec, xyz, xyz64 out
         "pair_plan": 64 * int(np.ceil(len(sa) / 128)),   # one 64-byte plan per tile
         "pair_kernel": 64 * kept_a + 64 * kept_b + 24 * n_match,   # both segments once, pairs out
     }
@@ -324,9 +331,22 @@ def run_ours(args):
         gbs = alg_bytes[k] / (t * 1e-3) / 1e9 if t > 0 else 0.0
         stages[k] = {"ms": t, "alg_bytes": alg_bytes[k], "GB/s": gbs, "frac": gbs / hbm}
     dom = max(per, key=per.get)
+    # DRAM bytes (read + write) per launch from one ncu capture of the same kernels on the config-1 catalogs
+    # cut to dec 0..10 deg (same objects per zone; profiles/build_and_pair_kernels_config1_band.md),
+    # scaled by the objects a launch processes
+    band_a = 4_397_838
+    traffic_per_obj = {"pair_kernel": (595.95e6 + 69.23e6) / band_a, "zb_scatter": (105.69e6 + 89.51e6) / band_a,
+                       "zb_zone_sort": (237.64e6 + 368.32e6) / band_a, "pair_plan": 3.01e6 / band_a}
+    units = {"pair_kernel": kept_a, "pair_plan": kept_a, "zb_scatter": nc, "zb_zone_sort": nc}
+    for k in stages:
+        if k in traffic_per_obj:
+            stages[k]["traffic"] = traffic_per_obj[k] * units[k]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": stages[dom]["GB/s"], "peak": hbm, "unit": "GB/s",
-                "frac": stages[dom]["frac"], "traffic": None, "peak_source": peak_kind}
-    pipeline_bytes = 2 * (24 + 64) * n + 64 * (kept_a + kept_b) + 24 * n_match
+                "frac": stages[dom]["frac"], "traffic": stages[dom].get("traffic"),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per object on a dec-band cut of "
+                                  "the same catalogs, times the objects of this launch",
+                "peak_source": peak_kind}
+    pipeline_bytes = (24 + 64) * (n + nb) + 64 * (kept_a + kept_b) + 24 * n_match
     pipeline = {"alg_bytes": pipeline_bytes, "GB/s": pipeline_bytes / (ms * 1e-3) / 1e9,
                 "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / hbm}
     value = world * n_cand / (ms * 1e-3)
@@ -398,11 +418,12 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded config1 mixture; no survey data)",
-        "config": {"workload": "config1 50Mx50M full-scale single pass, r=zh=1\"" if n == 50_000_000 else
-                   "config1 mixture %d x %d, r=zh=1\"" % (n, n),
+        "config": {"workload": "config1 50Mx50M full-scale single pass, r=zh=1\"" if n == nb == 50_000_000 else
+                   "config1 mixture %d x %d, r=zh=1\"%s" % (n, nb, " (dec band %g..%g deg of %d)" % (
+                       args.dec_band[0], args.dec_band[1], args.n) if args.dec_band else ""),
                    "n_per_catalog": n, "r_arcsec": 1.0, "zh_arcsec": 1.0, "variant": args.variant,
                    "parallelism": "replicas x%d" % world,
-                   "l2": "inputs (2 x %.1f GB records) larger than L2 (126 MB); no flush" % (24 * n / 1e9),
+                   "l2": "inputs (2 x %.1f GB records) larger than L2 (126 MB); no flush" % (24 * nc / 1e9),
                    "step": "zone build A + zone build B + pair kernel (inputs resident in HBM)"},
         "seconds_per_step": ms * 1e-3, "candidates": n_cand, "matches": n_match,
         "matches_per_s": world * n_match / (ms * 1e-3),
@@ -413,7 +434,7 @@ def run_ours(args):
         "roofline": roofline, "stages": stages, "pipeline_roofline": pipeline,
         "clocks": clocks,
         "e2e": {"value": world * n_cand / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": (24 if args.e2e_dist else 16) * n_match,
+                "h2d_bytes_per_step": 24 * (n + nb), "d2h_bytes_per_step": (24 if args.e2e_dist else 16) * n_match,
                 "path": "xm_segment_build(host) x2 + xm_match to host %s, pinned host buffers"
                         % ("{idA, idB, dist} records" if args.e2e_dist else
                            "{idA, idB} records (the reference's output record)"),
