@@ -180,6 +180,21 @@ def cpu_baseline(A, B, r_deg, target_s, steps=1):
             "matches": len(p)}
 
 
+def max_over_ranks(v, pg, device):
+    """The largest of every rank's value (the whole job ends when its slowest rank does)."""
+    if not pg:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, ms):
+    """Units per second of the whole job: every rank processes units_per_rank (replicas)."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -301,11 +316,8 @@ def run_ours(args):
     e1.synchronize()
     torch.cuda.synchronize(dev)
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, pg, dev)
     if pg:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
         torch.distributed.barrier()
     K = args.steps
     per = {
@@ -349,7 +361,7 @@ def run_ours(args):
     pipeline_bytes = (24 + 64) * (n + nb) + 64 * (kept_a + kept_b) + 24 * n_match
     pipeline = {"alg_bytes": pipeline_bytes, "GB/s": pipeline_bytes / (ms * 1e-3) / 1e9,
                 "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / hbm}
-    value = world * n_cand / (ms * 1e-3)
+    value = whole_job_rate(world, n_cand, ms)
 
     # ---- e2e through the C ABI with host buffers ----
     e2e_steps = args.e2e_steps or max(1, min(args.steps, 3))
@@ -406,11 +418,7 @@ def run_ours(args):
         got = e2e_step()
     f1.record(stream)
     f1.synchronize()
-    e2e_ms = f0.elapsed_time(f1) / e2e_steps
-    if pg:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1) / e2e_steps, pg, dev)
     if got != n_match:
         raise RuntimeError("e2e match count %d differs from %d" % (got, n_match))
 
@@ -426,14 +434,14 @@ def run_ours(args):
                    "l2": "inputs (2 x %.1f GB records) larger than L2 (126 MB); no flush" % (24 * nc / 1e9),
                    "step": "zone build A + zone build B + pair kernel (inputs resident in HBM)"},
         "seconds_per_step": ms * 1e-3, "candidates": n_cand, "matches": n_match,
-        "matches_per_s": world * n_match / (ms * 1e-3),
+        "matches_per_s": whole_job_rate(world, n_match, ms),
         "tested_pairs": stats.n_tested // K, "fp64_decisions": stats.n_exact // K,
         "border_pairs": stats.n_border // K,
         "borderline_fraction": (stats.n_border / stats.n_tested) if stats.n_tested else 0.0,
         "gpu_launches": int(stats.n_launches),
         "roofline": roofline, "stages": stages, "pipeline_roofline": pipeline,
         "clocks": clocks,
-        "e2e": {"value": world * n_cand / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
+        "e2e": {"value": whole_job_rate(world, n_cand, e2e_ms), "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 24 * (n + nb), "d2h_bytes_per_step": (24 if args.e2e_dist else 16) * n_match,
                 "path": "xm_segment_build(host) x2 + xm_match to host %s, pinned host buffers"
                         % ("{idA, idB, dist} records" if args.e2e_dist else
