@@ -68,6 +68,12 @@ def build(verbose=False, force=False):
                 print(o)
     if force or jobs or _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread"])
+    # command-line driver (xm_cli.cpp) linked against the library, found next to it at run time
+    cli_src = os.path.join(CSRC, "xm_cli.cpp")
+    if force or _stale(CLI, [cli_src, LIB] + headers):
+        os.makedirs(os.path.dirname(CLI), exist_ok=True)
+        _run(["g++"] + CXXFLAGS + [cli_src, "-o", CLI, "-L" + HERE, "-lxmatch_b200", "-Wl,-rpath,$ORIGIN/..",
+                                   "-lpthread"])
     return LIB
 
 
