@@ -598,21 +598,40 @@ __device__ __forceinline__ void store_plan(TilePlan *dst, const TilePlan &P)
 }
 
 // Cuts work item `item` into tiles (see the file header); calls f(start, len, zf, zl).
+// Zone offsets of A and B and RA half-widths of A's zones, read from shared
+// memory when a work item's slice is cached there, else from the job's arrays.
+struct ZoneView {
+    const uint32_t *azo;
+    int az0;               // a_zoff[z] = azo[z - az0]
+    const uint32_t *bzo;
+    int bz0;
+    const double *al;
+    int al0;
+    __device__ __forceinline__ uint32_t a(int z) const { return azo[z - az0]; }
+    __device__ __forceinline__ uint32_t b(int z) const { return bzo[z - bz0]; }
+    __device__ __forceinline__ double alpha(int z) const { return al[z - al0]; }
+};
+
+__device__ __forceinline__ ZoneView global_view(const JobDev &J)
+{
+    return ZoneView{J.a_zoff, 0, J.b_zoff, 0, J.alpha, J.alpha_z0};
+}
+
 template <class F>
-__device__ __forceinline__ void for_each_tile(const JobDev &J, uint32_t item, uint32_t zc, uint32_t tile, F f)
+__device__ __forceinline__ void for_each_tile(const JobDev &J, const ZoneView &V, uint32_t item, uint32_t zc,
+                                              uint32_t tile, F f)
 {
     const int z0 = J.z_lo + (int)((item - J.item_begin) * zc);
     const int z1 = min(z0 + (int)zc, J.z_hi + 1);
-    const uint32_t *zo = J.a_zoff;
     int z = z0;
-    uint32_t pos = zo[z0];
+    uint32_t pos = V.a(z0);
     while (true) {
-        while (z < z1 && pos >= zo[z + 1]) {
+        while (z < z1 && pos >= V.a(z + 1)) {
             ++z;
-            pos = max(pos, zo[z]);
+            pos = max(pos, V.a(z));
         }
         if (z >= z1) return;
-        const uint32_t zb0 = zo[z], zb1 = zo[z + 1];
+        const uint32_t zb0 = V.a(z), zb1 = V.a(z + 1);
         const uint32_t cnt = zb1 - zb0;
         if (cnt > tile / 2) {            // large zone: near-equal single-zone tiles
             const uint32_t k = (cnt + tile - 1) / tile;
@@ -625,8 +644,8 @@ __device__ __forceinline__ void for_each_tile(const JobDev &J, uint32_t item, ui
             uint32_t end = zb1;
             int zl = z, zn = z + 1;
             while (zn < z1) {
-                const uint32_t e1 = zo[zn + 1];
-                const uint32_t c1 = e1 - zo[zn];
+                const uint32_t e1 = V.a(zn + 1);
+                const uint32_t c1 = e1 - V.a(zn);
                 if (c1 > tile / 2 || e1 - start > tile) break;
                 if (c1 > 0) {
                     zl = zn;
@@ -646,14 +665,14 @@ __device__ __forceinline__ void for_each_tile(const JobDev &J, uint32_t item, ui
 // at most cap_b objects, each staged and tested as its own plan; pieces go
 // to the "heavy" queue that the pair kernel hands out first, one at a time.
 // Returns the number of pieces (1 = not split) and the piece size.
-__device__ __forceinline__ uint32_t tile_pieces(const JobDev &J, uint32_t len, int zf, int zl, uint32_t cap_b,
-                                                uint32_t *piece)
+__device__ __forceinline__ uint32_t tile_pieces(const JobDev &J, const ZoneView &V, uint32_t len, int zf, int zl,
+                                                uint32_t cap_b, uint32_t *piece)
 {
     const int band_lo = max(0, zf - J.nz), band_hi = min(J.n_zones - 1, zl + J.nz);
     const uint32_t nseg = (uint32_t)(band_hi - band_lo + 1);
-    const uint32_t b_len = J.b_zoff[band_hi + 1] - J.b_zoff[band_lo];
+    const uint32_t b_len = V.b(band_hi + 1) - V.b(band_lo);
     *piece = b_len;
-    const bool full_ring = J.alpha[zf - J.alpha_z0] >= 3.0 || J.alpha[zl - J.alpha_z0] >= 3.0;
+    const bool full_ring = V.alpha(zf) >= 3.0 || V.alpha(zl) >= 3.0;
     if (!full_ring || (int)nseg > kMaxBand || (uint64_t)len * b_len <= kHeavyPairs) return 1;
     uint32_t pc = max(32u, kHeavyPairs / max(len, 1u));
     pc = min(pc, cap_b);
@@ -676,9 +695,10 @@ __global__ void tiles_count(const JobDev *__restrict__ jobs, int n_jobs, uint32_
     if (item >= n_items) return;
     const JobDev &J = jobs[n_jobs > 1 ? find_job(jobs, n_jobs, item) : 0];
     uint32_t c = 0, h = 0;
-    for_each_tile(J, item, zc, tile, [&](uint32_t, uint32_t len, int zf, int zl) {
+    const ZoneView V = global_view(J);
+    for_each_tile(J, V, item, zc, tile, [&](uint32_t, uint32_t len, int zf, int zl) {
         uint32_t piece;
-        const uint32_t n = tile_pieces(J, len, zf, zl, cap_b, &piece);
+        const uint32_t n = tile_pieces(J, V, len, zf, zl, cap_b, &piece);
         if (n > 1) h += n; else ++c;
     });
     cnt[item] = c;
@@ -686,19 +706,45 @@ __global__ void tiles_count(const JobDev *__restrict__ jobs, int n_jobs, uint32_
 }
 
 // Plans: heavy pieces first (off[n_items + item] within [0, n_heavy)), then the
-// normal ones (n_heavy + off[item]).
-__global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32_t zc, uint32_t tile,
-                           uint32_t cap_b, const uint32_t *__restrict__ off_n, const uint32_t *__restrict__ off_h,
-                           TilePlan *__restrict__ plans, uint32_t max_tiles, unsigned long long *err)
+// normal ones (n_heavy + off[item]).  One warp per work item: the item's zone
+// offsets and RA half-widths are first loaded into shared memory by all lanes
+// at once, then every lane walks the tiles in step (uniform control flow, the
+// same values); lane 0 writes the normal plans, all lanes the heavy pieces.
+constexpr int kMakeWarps = 4;
+constexpr int kZcMax = 64;           // zones per work item at most (xm_run_jobs checks)
+constexpr int kBandCache = 224;      // B zone offsets cached per item
+
+__global__ void __launch_bounds__(32 * kMakeWarps)
+tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32_t zc, uint32_t tile, uint32_t cap_b,
+           const uint32_t *__restrict__ off_n, const uint32_t *__restrict__ off_h, TilePlan *__restrict__ plans,
+           uint32_t max_tiles, unsigned long long *err)
 {
-    const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
-    if (item >= n_items) return;
+    __shared__ uint32_t s_azo[kMakeWarps][kZcMax + 1];
+    __shared__ uint32_t s_bzo[kMakeWarps][kBandCache];
+    __shared__ double s_al[kMakeWarps][kZcMax];
+    const int w = threadIdx.x >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t item = blockIdx.x * kMakeWarps + w;
+    if (item >= n_items) return;   // whole warp
     const int jx = n_jobs > 1 ? find_job(jobs, n_jobs, item) : 0;
     const JobDev &J = jobs[jx];
+    const int z0 = J.z_lo + (int)((item - J.item_begin) * zc);
+    const int z1 = min(z0 + (int)zc, J.z_hi + 1);
+    const int nza = z1 - z0;
+    const int blo = max(0, z0 - J.nz), bhi = min(J.n_zones - 1, z1 - 1 + J.nz);
+    const int nbo = bhi + 2 - blo;   // B offsets [blo, bhi + 1]
+    ZoneView V = global_view(J);
+    if (nza <= kZcMax && nbo <= kBandCache) {
+        for (int k = lane; k <= nza; k += 32) s_azo[w][k] = __ldg(&J.a_zoff[z0 + k]);
+        for (int k = lane; k < nbo; k += 32) s_bzo[w][k] = __ldg(&J.b_zoff[blo + k]);
+        for (int k = lane; k < nza; k += 32) s_al[w][k] = __ldg(&J.alpha[z0 + k - J.alpha_z0]);
+        __syncwarp();
+        V = ZoneView{s_azo[w], z0, s_bzo[w], blo, s_al[w], z0};
+    }
     const uint32_t n_heavy = off_h[n_items];
     uint32_t o = n_heavy + off_n[item];
     uint32_t oh = off_h[item];
-    for_each_tile(J, item, zc, tile, [&](uint32_t start, uint32_t len, int zf, int zl) {
+    for_each_tile(J, V, item, zc, tile, [&](uint32_t start, uint32_t len, int zf, int zl) {
         TilePlan P;
         P.a_start = start;
         P.a_len = len;
@@ -707,30 +753,31 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
         P.band_lo = band_lo;
         P.zf = zf;
         const uint32_t nseg = (uint32_t)(band_hi - band_lo + 1);
-        const uint32_t B0 = J.b_zoff[band_lo], B1 = J.b_zoff[band_hi + 1];
+        const uint32_t B0 = V.b(band_lo), B1 = V.b(band_hi + 1);
         P.b_start = B0;
         P.b_len = B1 - B0;
         for (int k = 0; k < kMaxPlanSeg; ++k) P.seg_g[k] = P.seg_len[k] = 0;
         const uint32_t zword = (min(nseg, 255u) << 8) | ((uint32_t)(zl - zf) << 16);
         uint32_t piece;
-        const uint32_t npc = tile_pieces(J, len, zf, zl, cap_b, &piece);
+        const uint32_t npc = tile_pieces(J, V, len, zf, zl, cap_b, &piece);
         if (npc > 1) {
-            // heavy: WHOLE plans over consecutive B pieces of the band
-            for (uint32_t q = 0; q < npc; ++q) {
-                P.b_start = B0 + q * piece;
-                P.b_len = min(piece, B1 - P.b_start);
-                P.mode = PLAN_WHOLE | zword;
-                if (oh < max_tiles) store_plan(plans + oh, P);
+            // heavy: WHOLE plans over consecutive B pieces of the band, one per lane
+            P.mode = PLAN_WHOLE | zword;
+            for (uint32_t q = lane; q < npc; q += 32) {
+                TilePlan Q = P;
+                Q.b_start = B0 + q * piece;
+                Q.b_len = min(piece, B1 - Q.b_start);
+                if (oh + q < max_tiles) store_plan(plans + oh + q, Q);
                 else atomicExch(err, 1ull);
-                ++oh;
             }
+            oh += npc;
             return;
         }
         uint32_t mode = PLAN_GLOBAL;
         if ((int)nseg <= kMaxBand && P.b_len <= cap_b) {
             mode = PLAN_WHOLE;
-        } else if (zf == zl && (int)nseg <= kMaxPlanSeg && J.alpha[zf - J.alpha_z0] < 3.0) {
-            const double alpha = J.alpha[zf - J.alpha_z0];
+        } else if (zf == zl && (int)nseg <= kMaxPlanSeg && V.alpha(zf) < 3.0) {
+            const double alpha = V.alpha(zf);
             // A is ordered by raq: every tile object's ra is within one raq step q of
             // [ra_first, ra_last]; widen by 2q
             const double q2 = 2.0 * ldexp(XM_TWO_PI, J.raq_shift - 32);
@@ -744,7 +791,7 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
 #pragma unroll
             for (int k = 0; k < kMaxPlanSeg; ++k) {
                 if (k >= (int)nseg) break;
-                const uint32_t b0 = J.b_zoff[band_lo + k], b1 = J.b_zoff[band_lo + k + 1];
+                const uint32_t b0 = V.b(band_lo + k), b1 = V.b(band_lo + k + 1);
                 uint32_t sb = b0, ln = b1 - b0;
                 if (ln > 0) {
                     const bool wrap = !(t_hi2 < raq_at_g(J.b_xyz, b0) && t_lo3 > raq_at_g(J.b_xyz, b1 - 1));
@@ -764,8 +811,10 @@ __global__ void tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t
         }
         // nseg is only read for WHOLE (<= kMaxBand) and UNION (<= kMaxPlanSeg) plans
         P.mode = mode | zword;
-        if (o < max_tiles) store_plan(plans + o, P);
-        else atomicExch(err, 1ull);
+        if (lane == 0) {
+            if (o < max_tiles) store_plan(plans + o, P);
+            else atomicExch(err, 1ull);
+        }
         ++o;
     });
 }
@@ -1233,8 +1282,8 @@ cudaError_t plan_count(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint3
 cudaError_t plan_make(const LaunchCfg &L, const JobDev *jobs, int n_jobs, uint32_t n_items, const uint32_t *off,
                       uint32_t n_normal, uint32_t n_heavy, void *plans, unsigned long long *err, cudaStream_t st)
 {
-    const unsigned g = (n_items + 127) / 128;
-    tiles_make<<<g, 128, 0, st>>>(jobs, n_jobs, n_items, L.zc, (uint32_t)L.tile, 4u * (uint32_t)L.tile, off,
+    const unsigned g = (n_items + kMakeWarps - 1) / kMakeWarps;
+    tiles_make<<<g, 32 * kMakeWarps, 0, st>>>(jobs, n_jobs, n_items, L.zc, (uint32_t)L.tile, 4u * (uint32_t)L.tile, off,
                                   off + n_items + 1, (TilePlan *)plans, n_normal + n_heavy, err);
     return cudaGetLastError();
 }
