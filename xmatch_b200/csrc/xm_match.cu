@@ -148,16 +148,25 @@ struct Win {
     uint32_t lo3, hi3;   // branch 3 (B near 2 pi)
 };
 
+// The wraparound windows are empty (lo > hi) unless the direct window crosses
+// ra = 2 pi (branch 2: B with ra < hi - 2 pi) or ra = 0 (branch 3: B with
+// ra > lo + 2 pi); ra of a kept object lies in [0, 2 pi).
 __device__ __forceinline__ Win make_win(double ra, double alpha, int shift)
 {
     const double lo = ra - alpha - kWinEps, hi = ra + alpha + kWinEps;
     Win w;
     w.lo = xm::raq32(lo) >> shift;
     w.hi = xm::raq32(hi) >> shift;
-    w.lo2 = xm::raq32(lo - XM_TWO_PI - kWinEps) >> shift;
-    w.hi2 = xm::raq32(hi - XM_TWO_PI + kWinEps) >> shift;
-    w.lo3 = xm::raq32(lo + XM_TWO_PI - kWinEps) >> shift;
-    w.hi3 = xm::raq32(hi + XM_TWO_PI + kWinEps) >> shift;
+    w.lo2 = w.lo3 = 0xFFFFFFFFu;
+    w.hi2 = w.hi3 = 0u;
+    if (hi - XM_TWO_PI + kWinEps > 0.0) {
+        w.lo2 = xm::raq32(lo - XM_TWO_PI - kWinEps) >> shift;
+        w.hi2 = xm::raq32(hi - XM_TWO_PI + kWinEps) >> shift;
+    }
+    if (lo - kWinEps < 0.0) {
+        w.lo3 = xm::raq32(lo + XM_TWO_PI - kWinEps) >> shift;
+        w.hi3 = xm::raq32(hi + XM_TWO_PI + kWinEps) >> shift;
+    }
     return w;
 }
 
@@ -466,12 +475,12 @@ __device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, 
             const uint32_t j0 = lower_v(V, b0, b1, w.lo);
             const uint32_t j1 = upper_v(V, j0, b1, w.hi);
             XM_PUSH(j0, j1);
-            if (w.hi2 >= raq_at(V.xyz, b0)) {
+            if (w.lo2 <= w.hi2 && w.hi2 >= raq_at(V.xyz, b0)) {
                 const uint32_t w0 = lower_v(V, b0, j0, w.lo2);
                 const uint32_t w1 = upper_v(V, w0, j0, w.hi2);
                 XM_PUSH(w0, w1);
             }
-            if (w.lo3 <= raq_at(V.xyz, b1 - 1)) {
+            if (w.lo3 <= w.hi3 && w.lo3 <= raq_at(V.xyz, b1 - 1)) {
                 const uint32_t w0 = lower_v(V, j1, b1, w.lo3);
                 const uint32_t w1 = upper_v(V, w0, b1, w.hi3);
                 XM_PUSH(w0, w1);
