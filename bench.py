@@ -49,8 +49,9 @@ def parse():
     ap.add_argument("--n", type=int, default=50_000_000, help="sources per catalog")
     ap.add_argument("--variant", default="filter32", choices=["filter32", "plain64"])
     ap.add_argument("--e2e-steps", type=int, default=None)
-    ap.add_argument("--e2e-dist", action="store_true",
-                    help="e2e also returns distances (24-byte records instead of the reference's 16-byte pairs)")
+    ap.add_argument("--dist", "--e2e-dist", dest="dist", action="store_true",
+                    help="also compute and return distances (24-byte records instead of the reference's "
+                         "16-byte {idA, idB} pairs)")
     ap.add_argument("--dec-band", type=float, nargs=2, default=None, metavar=("LO", "HI"),
                     help="keep only sources with dec in [LO, HI) deg (same density, smaller case for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -295,7 +296,7 @@ def run_ours(args):
     def step(stats):
         sa.rebuild_device(dA.data_ptr(), n, stats)
         sb.rebuild_device(dB.data_ptr(), nb, stats)
-        ms_ = ctx.match(sa, sb, r, flags, fetch=False)[2]
+        ms_ = ctx.match(sa, sb, r, flags, fetch=False, with_dist=args.dist)[2]
         for k in ("ms_match", "ms_plan", "n_tested", "n_exact", "n_border", "n_launches"):
             setattr(stats, k, getattr(stats, k) + ms_[k])
 
@@ -334,7 +335,9 @@ def run_ours(args):
         "zb_scatter": (24 + 32) * nc,              # records in, 32-byte bucket records out
         "zb_zone_sort": (32 + 64) * nc,            # bucket records in; id, radec, xyz, xyz64 out
         "pair_plan": 64 * int(np.ceil(len(sa) / 128)),   # one 64-byte plan per tile
-        "pair_kernel": 64 * kept_a + 64 * kept_b + 24 * n_match,   # both segments once, pairs out
+        # both segments once (id, radec, FP32 xyz), pairs out; with distances also the FP64
+        # vectors of both ends of every match
+        "pair_kernel": 40 * (kept_a + kept_b) + (16 + 8 + 48 if args.dist else 16) * n_match,
     }
     peaks, peak_kind = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
@@ -358,7 +361,7 @@ def run_ours(args):
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per object on a dec-band cut of "
                                   "the same catalogs, times the objects of this launch",
                 "peak_source": peak_kind}
-    pipeline_bytes = (24 + 64) * (n + nb) + 64 * (kept_a + kept_b) + 24 * n_match
+    pipeline_bytes = (24 + 64) * (n + nb) + 40 * (kept_a + kept_b) + (24 if args.dist else 16) * n_match
     pipeline = {"alg_bytes": pipeline_bytes, "GB/s": pipeline_bytes / (ms * 1e-3) / 1e9,
                 "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / hbm}
     value = whole_job_rate(world, n_cand, ms)
@@ -387,8 +390,8 @@ def run_ours(args):
         t1 = time.perf_counter()
         s2 = ctx.build(objB, zh, 1, bs)
         t2 = time.perf_counter()
-        p, d, st = ctx.match(s1, s2, r, flags, with_dist=args.e2e_dist,
-                             out=(outP, outD if args.e2e_dist else None))
+        p, d, st = ctx.match(s1, s2, r, flags, with_dist=args.dist,
+                             out=(outP, outD if args.dist else None))
         t3 = time.perf_counter()
         s1.free()
         s2.free()
@@ -432,7 +435,9 @@ def run_ours(args):
                    "n_per_catalog": n, "r_arcsec": 1.0, "zh_arcsec": 1.0, "variant": args.variant,
                    "parallelism": "replicas x%d" % world,
                    "l2": "inputs (2 x %.1f GB records) larger than L2 (126 MB); no flush" % (24 * nc / 1e9),
-                   "step": "zone build A + zone build B + pair kernel (inputs resident in HBM)"},
+                   "step": "zone build A + zone build B + pair kernel (inputs resident in HBM)",
+                   "output": "{idA, idB, dist} per match" if args.dist else
+                             "{idA, idB} per match, the reference's output record (--dist adds distances)"},
         "seconds_per_step": ms * 1e-3, "candidates": n_cand, "matches": n_match,
         "matches_per_s": whole_job_rate(world, n_match, ms),
         "tested_pairs": stats.n_tested // K, "fp64_decisions": stats.n_exact // K,
@@ -442,9 +447,9 @@ def run_ours(args):
         "roofline": roofline, "stages": stages, "pipeline_roofline": pipeline,
         "clocks": clocks,
         "e2e": {"value": whole_job_rate(world, n_cand, e2e_ms), "unit": UNIT, "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": 24 * (n + nb), "d2h_bytes_per_step": (24 if args.e2e_dist else 16) * n_match,
+                "h2d_bytes_per_step": 24 * (n + nb), "d2h_bytes_per_step": (24 if args.dist else 16) * n_match,
                 "path": "xm_segment_build(host) x2 + xm_match to host %s, pinned host buffers"
-                        % ("{idA, idB, dist} records" if args.e2e_dist else
+                        % ("{idA, idB, dist} records" if args.dist else
                            "{idA, idB} records (the reference's output record)"),
                 "parts_ms": {k: v / e2e_steps for k, v in e2e_parts.items()}},
     }

@@ -533,25 +533,31 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
         bool m = false;
         double c2 = 0;
         const double2 rb = V.radec[q];
-        if (VARIANT == 0) {   // FP32 reject, FP64 decision
+        if (VARIANT == 0) {   // FP32 reject above thr_hi, accept below thr_lo, FP64 decision between
             if (COUNT_CAND) cn.cand += cuts_pass(J, a, rb) ? 1ull : 0ull;
             const float4 fb = V.xyz[q];
             const float dx = a.fx - fb.x, dy = a.fy - fb.y, dz = a.fz - fb.z;
             const float c32 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
             if (!(c32 > J.thr_hi)) {
-                cn.border += (c32 >= J.thr_lo) ? 1ull : 0ull;
-                cn.exact++;
+                const bool band = c32 >= J.thr_lo;
+                cn.border += band ? 1ull : 0ull;
                 if (cuts_pass(J, a, rb)) {
-                    if (!a.have_xyz) {
-                        a.x = __ldg(&J.a_xyz64[3 * (size_t)a.gi]);
-                        a.y = __ldg(&J.a_xyz64[3 * (size_t)a.gi + 1]);
-                        a.z = __ldg(&J.a_xyz64[3 * (size_t)a.gi + 2]);
-                        a.have_xyz = true;
+                    m = true;
+                    if (band || DIST) {
+                        if (!a.have_xyz) {
+                            a.x = __ldg(&J.a_xyz64[3 * (size_t)a.gi]);
+                            a.y = __ldg(&J.a_xyz64[3 * (size_t)a.gi + 1]);
+                            a.z = __ldg(&J.a_xyz64[3 * (size_t)a.gi + 2]);
+                            a.have_xyz = true;
+                        }
+                        const size_t gb = 3 * (size_t)global_index(V, c.zb, q);
+                        c2 = chord2(a.x, a.y, a.z, __ldg(&J.b_xyz64[gb]), __ldg(&J.b_xyz64[gb + 1]),
+                                    __ldg(&J.b_xyz64[gb + 2]));
+                        if (band) {
+                            cn.exact++;
+                            m = c2 < J.sr_dist2;
+                        }
                     }
-                    const size_t gb = 3 * (size_t)global_index(V, c.zb, q);
-                    c2 = chord2(a.x, a.y, a.z, __ldg(&J.b_xyz64[gb]), __ldg(&J.b_xyz64[gb + 1]),
-                                __ldg(&J.b_xyz64[gb + 2]));
-                    m = c2 < J.sr_dist2;
                 }
             }
         } else {              // plain all-FP64: cuts, then unit vectors by sincos per pair
@@ -1172,15 +1178,23 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                             const float dx = fa.x - fb.x, dy = fa.y - fb.y, dz = fa.z - fb.z;
                             const float c32 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                             if (!(c32 > K.thr_hi)) {
-                                cn.border += (c32 >= K.thr_lo) ? 1ull : 0ull;
-                                cn.exact++;
+                                // below thr_lo the FP64 chord is below the threshold (proven bound):
+                                // FP64 only inside the band, or for the distance
+                                const bool band = c32 >= K.thr_lo;
+                                cn.border += band ? 1ull : 0ull;
                                 if (cuts_k(K, ra.x, ra.y, al, rb)) {
-                                    const size_t ga = 3 * (size_t)(S.a_start + ta);
-                                    const size_t gb = 3 * (size_t)staged_global(V, (int)S.nseg, q);
-                                    c2 = chord2(__ldg(&J.a_xyz64[ga]), __ldg(&J.a_xyz64[ga + 1]), __ldg(&J.a_xyz64[ga + 2]),
-                                                __ldg(&J.b_xyz64[gb]), __ldg(&J.b_xyz64[gb + 1]),
-                                                __ldg(&J.b_xyz64[gb + 2]));
-                                    m = c2 < K.sr_dist2;
+                                    m = true;
+                                    if (band || DIST) {
+                                        const size_t ga = 3 * (size_t)(S.a_start + ta);
+                                        const size_t gb = 3 * (size_t)staged_global(V, (int)S.nseg, q);
+                                        c2 = chord2(__ldg(&J.a_xyz64[ga]), __ldg(&J.a_xyz64[ga + 1]),
+                                                    __ldg(&J.a_xyz64[ga + 2]), __ldg(&J.b_xyz64[gb]),
+                                                    __ldg(&J.b_xyz64[gb + 1]), __ldg(&J.b_xyz64[gb + 2]));
+                                        if (band) {
+                                            cn.exact++;
+                                            m = c2 < K.sr_dist2;
+                                        }
+                                    }
                                 }
                             }
                         } else {
