@@ -163,6 +163,15 @@ xm_status xm_match_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint3
 xm_status xm_autotune_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags,
                             xm_tuning *best, float *best_ms, float *fixed_ms);
 
+/* Crossmatch of two catalogs in host memory (the whole of _main for one pair,
+ * BoostXmatch.cpp:247-330, in one call): both are zone-built, B's host-to-device
+ * copy overlapping A's copy and build, then matched.  If out's buffers are
+ * pinned (cudaHostAlloc / cudaHostRegister) and hold every match, the pair
+ * kernel writes the matches straight into them; otherwise they are copied.
+ * XM_ERR_CAPACITY (out->count = matches) leaves the matches for xm_fetch_pairs. */
+xm_status xm_crossmatch(xm_ctx *ctx, const xm_obj *A, uint64_t nA, const xm_obj *B, uint64_t nB, double sr_deg,
+                        double zh_deg, uint32_t flags, xm_pairs *out, xm_stats *stats);
+
 /* ---- serving: a resident catalog answering a stream of query catalogs ----
  * Replaces the reference's run-to-completion driver (_main,
  * BoostXmatch.cpp:247-330, which loads, sorts and matches one catalog pair

@@ -287,6 +287,65 @@ def test_batch_of_many_radii(ctx):
         y.free()
 
 
+@pytest.mark.parametrize("pinned", [False, True])
+@pytest.mark.parametrize("with_dist", [True, False])
+def test_crossmatch_one_call(ctx, fixtures, pinned, with_dist):
+    # host records in, matches out; pinned output buffers are written by the pair kernel directly
+    import torch
+    import xmatch_b200 as xm
+    a, a2 = fixtures
+    r = 5 * ARCSEC
+    po, do, _ = oracle.xmatch(a2, a, r)
+    po, do = sp(po, do)
+    cap = len(po) + 100
+    if pinned:
+        P = torch.empty(cap * 2, dtype=torch.int64, pin_memory=True).numpy().reshape(-1, 2)
+        D = torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy() if with_dist else None
+    else:
+        P = np.empty((cap, 2), np.int64)
+        D = np.empty(cap, np.float64) if with_dist else None
+    p, d, st = ctx.crossmatch(a2, a, r, flags=xm.XM_FILTER32, with_dist=with_dist, out=(P, D))
+    if with_dist:
+        p, d = sp(p, d)
+        assert np.max(np.abs(d - do), initial=0) <= DIST_TOL
+    else:
+        p = sp(p)
+    assert np.array_equal(p, po)
+    assert st["n_match"] == len(po)
+    # output too small: the count is reported and the matches wait on the device
+    small = np.empty((10, 2), np.int64)
+    with pytest.raises(xm.XmatchError) as e:
+        ctx.crossmatch(a2, a, r, with_dist=False, out=(small, None))
+    assert e.value.status == xm._capi.XM_ERR_CAPACITY
+    q, _ = ctx.fetch(len(po), with_dist=False)
+    assert np.array_equal(sp(q), po)
+
+
+def test_crossmatch_streams_a_in_chunks(ctx, fixtures, monkeypatch):
+    # 2,000-object chunks: A (10,000) streamed in 5 chunks through 2 staging slots
+    import torch
+    monkeypatch.setenv("XMATCH_CHUNK_OBJS", "2000")
+    a, a2 = fixtures
+    r = 5 * ARCSEC
+    po, do, _ = oracle.xmatch(a, a2, r)
+    po, do = sp(po, do)
+    cap = len(po) + 10
+    P = torch.empty(cap * 2, dtype=torch.int64, pin_memory=True).numpy().reshape(-1, 2)
+    D = torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy()
+    for _ in range(2):
+        p, d, st = ctx.crossmatch(a, a2, r, out=(P, D))
+        p, d = sp(p, d)
+        assert np.array_equal(p, po) and np.max(np.abs(d - do), initial=0) <= DIST_TOL
+    # room for fewer than all: the whole match reruns into device buffers, the count is reported
+    import xmatch_b200 as xm
+    with pytest.raises(xm.XmatchError) as e:
+        ctx.crossmatch(a, a2, r, out=(P[: len(po) // 2], D[: len(po) // 2]))
+    assert e.value.status == xm._capi.XM_ERR_CAPACITY
+    q, dq = ctx.fetch(len(po))
+    q, dq = sp(q, dq)
+    assert np.array_equal(q, po)
+
+
 def test_segmentation_invariance(ctx, fixtures):
     a, _ = fixtures
     whole, _, _ = oracle.xmatch(a, a, 5 * ARCSEC)

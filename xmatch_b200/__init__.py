@@ -312,6 +312,33 @@ class Context:
                                       ctypes.byref(fms)), self._h)
         return (best.tile, best.chunk, best.blocks_per_sm, best.zones), bms.value, fms.value
 
+    def crossmatch(self, A, B, sr_deg, zh_deg=None, flags=XM_FILTER32, with_dist=True, out=None):
+        """Both catalogs from host records to matches (xm_crossmatch): (pairs, dist, stats).
+        `out` = (pairs[n,2] int64, dist[n] or None); pinned arrays (e.g. from torch's
+        pin_memory) are written by the pair kernel directly."""
+        A, B = as_objs(A), as_objs(B)
+        if not with_dist:
+            flags |= XM_NO_DIST
+        if out is not None:
+            pairs, dist = out
+        else:
+            cap = 2 * max(len(A), len(B), 8)
+            pairs = np.empty((cap, 2), np.int64)
+            dist = np.empty(cap, np.float64) if with_dist else None
+        st = XmStats()
+        p = XmPairs(_ptr(pairs), _ptr(dist) if with_dist else None, len(pairs), 0)
+        rc = _lib.xm_crossmatch(self._h, _ptr(A), len(A), _ptr(B), len(B), sr_deg, zh_deg or sr_deg, flags,
+                                ctypes.byref(p), ctypes.byref(st))
+        if rc == _capi.XM_ERR_CAPACITY and out is None:
+            n = p.count
+            pairs = np.empty((n, 2), np.int64)
+            dist = np.empty(n, np.float64) if with_dist else None
+            p = XmPairs(_ptr(pairs), _ptr(dist) if with_dist else None, n, 0)
+            rc = _lib.xm_fetch_pairs(self._h, ctypes.byref(p))
+        _check(rc, self._h)
+        n = p.count
+        return pairs[:n], (dist[:n] if with_dist else None), st.as_dict()
+
     def unit_vectors(self, ra_deg, dec_deg):
         ra = np.ascontiguousarray(ra_deg, np.float64)
         de = np.ascontiguousarray(dec_deg, np.float64)
@@ -326,12 +353,7 @@ def crossmatch(A, B, r_arcsec, zh_arcsec=None, device=0, flags=XM_FILTER32, ctx=
     own = ctx is None
     ctx = ctx or Context(device)
     try:
-        sa = ctx.build(A, zh, 0)
-        sb = ctx.build(B, zh, 1)
-        out = ctx.match(sa, sb, r_arcsec / 3600.0, flags)
-        sa.free()
-        sb.free()
-        return out
+        return ctx.crossmatch(A, B, r_arcsec / 3600.0, zh, flags)
     finally:
         if own:
             ctx.close()

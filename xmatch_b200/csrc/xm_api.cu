@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -168,6 +169,10 @@ extern "C" xm_status xm_ctx_create(int device, xm_ctx **out)
     if ((e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
         return fail(e);
     if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreate(&ctx->ev_b2)) != cudaSuccess) return fail(e);
+    for (auto &ev : ctx->ev_slot)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
     props.handleTypes = cudaMemHandleTypeNone;
@@ -207,7 +212,15 @@ extern "C" xm_status xm_ctx_destroy(xm_ctx *ctx)
     xm_dev_free(ctx, ctx->d_plans);
     xm_dev_free(ctx, ctx->build_tmp);
     xm_dev_free(ctx, ctx->stage);
+    xm_dev_free(ctx, ctx->stage2);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->stream2) {
+        cudaStreamSynchronize(ctx->stream2);
+        cudaStreamDestroy(ctx->stream2);
+    }
+    if (ctx->ev_b2) cudaEventDestroy(ctx->ev_b2);
+    for (auto &ev : ctx->ev_slot)
+        if (ev) cudaEventDestroy(ev);
     if (ctx->counters) cudaFree(ctx->counters);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
     if (ctx->h_tiles) cudaFreeHost(ctx->h_tiles);
@@ -569,8 +582,9 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
 // Runs the pair kernel over the jobs; on return ctx->res holds the matches
 // (ungrouped) and ctx->h_counters the statistics.
 xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags, const xm_tuning *tuning,
-                      bool want_job, xm_stats *stats, float *kernel_ms)
+                      bool want_job, xm_stats *stats, float *kernel_ms, const xm_pairs *direct, bool *direct_used)
 {
+    if (direct_used) *direct_used = false;
     cudaStream_t st = ctx->stream;
     xm::LaunchCfg L;
     L.sm_count = ctx->sm_count;
@@ -645,6 +659,12 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
         out.dist = L.dist ? ctx->res.dist : nullptr;
         out.job = want_job ? ctx->res.job : nullptr;
         out.cap = ctx->res.cap;
+        const bool to_host = direct && retries == 0 && !want_job;
+        if (to_host) {   // straight into the caller's pinned buffers
+            out.pairs = (long long *)direct->pairs;
+            out.dist = L.dist ? (double *)direct->dist : nullptr;
+            out.cap = direct->capacity;
+        }
         out.counters = ctx->counters;
         // counters cleared, tile plans, pair kernel, counters read back
         auto enqueue = [&](unsigned ev_flags) -> cudaError_t {
@@ -693,7 +713,16 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
             return XM_ERR_TIMEOUT;
         }
         uint64_t found = ctx->h_counters[0];
-        if (found <= ctx->res.cap) break;
+        if (to_host && found <= direct->capacity) {
+            if (direct_used) *direct_used = true;
+            break;
+        }
+        if (!to_host && found <= ctx->res.cap) break;
+        if (to_host) {   // did not fit the caller's buffers: again into device buffers
+            retries++;
+            XM_TRY(ensure_result(ctx, found + found / 16 + 1024, want_job));
+            continue;
+        }
         // never truncate: grow to the exact count and run again
         retries++;
         uint64_t want = found + found / 16 + 1024;
@@ -773,6 +802,176 @@ extern "C" xm_status xm_fetch_pairs(xm_ctx *ctx, xm_pairs *out)
     uint64_t total = ctx->res.count;
     xm_status rc = copy_out(ctx, p, d, n, out, nullptr);
     out->count = total;
+    return rc;
+}
+
+// Device-accessible address of a pinned host buffer, or null for pageable memory.
+static void *pinned_device_ptr(const void *p)
+{
+    if (!p) return nullptr;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
+static xm_status grow(xm_ctx *ctx, void **p, size_t *have, size_t need)
+{
+    if (*have >= need && *p) return XM_OK;
+    xm_dev_free(ctx, *p);
+    *p = nullptr;
+    *have = 0;
+    XM_TRY(xm_dev_alloc(ctx, p, need));
+    *have = need;
+    return XM_OK;
+}
+
+// Both catalogs from host memory to matches in host memory.
+//
+// With pinned output buffers (device-accessible) the work is pipelined:
+// B is copied and zone-built first; then A is streamed in chunks through two
+// staging slots, each chunk copied on the second stream while the previous one
+// is built and matched against B, its matches written by the pair kernel
+// straight into the caller's buffers (device-to-host traffic that overlaps the
+// next chunk's host-to-device copy).  Any subset of A can be matched against
+// the whole of B, so the pair set is that of one match.  If the matches do not
+// fit the buffers, or the buffers are pageable, the catalogs are built whole
+// and matched once (XM_ERR_CAPACITY then reports the count and leaves the
+// matches for xm_fetch_pairs).
+namespace {
+// A objects per chunk at least (environment XMATCH_CHUNK_OBJS overrides it).  A chunk is
+// a slice of A's records in input order, so it spans all of A's zones and its match
+// walks all of B's: few large chunks (12M objects: 49 ms at 50M x 50M against 59 ms
+// for one, 53 ms for 6) balance that against the overlap.
+uint64_t chunk_objs()
+{
+    const char *e = std::getenv("XMATCH_CHUNK_OBJS");
+    const unsigned long long v = e ? std::strtoull(e, nullptr, 10) : 0ull;
+    return v ? (uint64_t)v : 12000000ull;   // 4 chunks at 50M: each chunk re-walks B's zones
+}
+}
+
+static xm_status crossmatch_whole(xm_ctx *ctx, const xm_obj *A, uint64_t nA, xm_segment *sb, double sr_deg,
+                                  double zh_deg, uint32_t flags, xm_pairs *out, xm_stats *stats)
+{
+    cudaStream_t st = ctx->stream;
+    XM_TRY(grow(ctx, &ctx->stage, &ctx->stage_bytes, std::max<uint64_t>(nA, 1) * sizeof(xm_obj)));
+    if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[12], st));
+    if (nA) XM_CUDA(ctx, cudaMemcpyAsync(ctx->stage, A, nA * sizeof(xm_obj), cudaMemcpyHostToDevice, st));
+    if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[13], st));
+    xm_segment *sa = nullptr;
+    xm_status rc = new_segment(ctx, 0, zh_deg, &sa);
+    if (rc == XM_OK) rc = xm_build_impl(sa, (const xm_obj *)ctx->stage, nA, stats);
+    if (rc == XM_OK && stats) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ctx->ev[12], ctx->ev[13]);
+        stats->ms_h2d += t;
+    }
+    if (rc == XM_OK) {
+        xm_job job = {sa, sb, sr_deg};
+        rc = xm_run_jobs(ctx, &job, 1, flags, nullptr, false, stats, nullptr);
+        if (rc == XM_OK && out) rc = copy_out(ctx, ctx->res.pairs, ctx->res.dist, ctx->res.count, out, stats);
+    }
+    xm_segment_free(sa);
+    return rc;
+}
+
+extern "C" xm_status xm_crossmatch(xm_ctx *ctx, const xm_obj *A, uint64_t nA, const xm_obj *B, uint64_t nB,
+                                   double sr_deg, double zh_deg, uint32_t flags, xm_pairs *out, xm_stats *stats)
+{
+    if (!ctx || (nA && !A) || (nB && !B) || !(zh_deg > 0)) return XM_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    cudaStream_t st = ctx->stream, s2 = ctx->stream2;
+    XM_CUDA(ctx, cudaEventRecord(ctx->ev[6], st));
+    // B: copied and built whole
+    XM_TRY(grow(ctx, &ctx->stage2, &ctx->stage2_bytes, std::max<uint64_t>(nB, 1) * sizeof(xm_obj)));
+    XM_CUDA(ctx, cudaEventRecord(ctx->ev[1], st));
+    if (nB) XM_CUDA(ctx, cudaMemcpyAsync(ctx->stage2, B, nB * sizeof(xm_obj), cudaMemcpyHostToDevice, st));
+    XM_CUDA(ctx, cudaEventRecord(ctx->ev_b2, st));
+    // the output route
+    const bool want_dist = (flags & XM_NO_DIST) == 0;
+    xm_pairs direct = {nullptr, nullptr, 0, 0};
+    if (out && out->pairs && (!out->dist || want_dist)) {
+        direct.pairs = (int64_t *)pinned_device_ptr(out->pairs);
+        direct.dist = want_dist ? (double *)pinned_device_ptr(out->dist) : nullptr;
+        direct.capacity = out->capacity;
+    }
+    const bool streamed = direct.pairs && (!want_dist || direct.dist);
+    const uint64_t n_chunks = streamed ? std::max<uint64_t>(1, std::min<uint64_t>(16, nA / chunk_objs())) : 1;
+    const uint64_t chunk = n_chunks > 1 ? (nA + n_chunks - 1) / n_chunks : nA;
+    // A chunks land in two slots of the staging buffer, copied on the second stream
+    XM_TRY(grow(ctx, &ctx->stage, &ctx->stage_bytes, 2 * std::max<uint64_t>(chunk, 1) * sizeof(xm_obj)));
+    xm_obj *slot[2] = {(xm_obj *)ctx->stage, (xm_obj *)ctx->stage + std::max<uint64_t>(chunk, 1)};
+    cudaEvent_t *landed = ctx->ev_slot;   // recorded only here
+    auto copy_chunk = [&](uint64_t c) -> xm_status {
+        const uint64_t first = c * chunk, n = std::min<uint64_t>(chunk, nA - first);
+        if (n) XM_CUDA(ctx, cudaMemcpyAsync(slot[c & 1], A + first, n * sizeof(xm_obj), cudaMemcpyHostToDevice, s2));
+        XM_CUDA(ctx, cudaEventRecord(landed[c & 1], s2));
+        return XM_OK;
+    };
+    xm_segment *sb = nullptr, *sa = nullptr;
+    xm_status rc = new_segment(ctx, 1, zh_deg, &sb);
+    if (rc == XM_OK && streamed) {
+        // A's first two chunks follow B on the link
+        if (cudaStreamWaitEvent(s2, ctx->ev_b2, 0) != cudaSuccess) rc = XM_ERR_CUDA;
+        if (rc == XM_OK) rc = copy_chunk(0);
+        if (rc == XM_OK && n_chunks > 1) rc = copy_chunk(1);
+    }
+    if (rc == XM_OK) rc = xm_build_impl(sb, (const xm_obj *)ctx->stage2, nB, stats);
+    if (rc == XM_OK && stats) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ctx->ev[1], ctx->ev_b2);
+        stats->ms_h2d += t;
+    }
+    if (rc == XM_OK && !streamed) {
+        rc = crossmatch_whole(ctx, A, nA, sb, sr_deg, zh_deg, flags, out, stats);
+    } else if (rc == XM_OK) {
+        uint64_t found = 0;
+        bool overflow = false;
+        rc = new_segment(ctx, 0, zh_deg, &sa);
+        for (uint64_t c = 0; rc == XM_OK && c < n_chunks; ++c) {
+            const uint64_t n = std::min<uint64_t>(chunk, nA - std::min<uint64_t>(nA, c * chunk));
+            if (cudaStreamWaitEvent(st, landed[c & 1], 0) != cudaSuccess) {
+                rc = XM_ERR_CUDA;
+                break;
+            }
+            rc = xm_build_impl(sa, slot[c & 1], n, stats);   // returns with the slot read (stream synchronised)
+            if (rc == XM_OK && c + 2 < n_chunks) rc = copy_chunk(c + 2);
+            if (rc != XM_OK) break;
+            xm_job job = {sa, sb, sr_deg};
+            xm_pairs dc = direct;
+            dc.pairs = direct.pairs + 2 * found;
+            dc.dist = direct.dist ? direct.dist + found : nullptr;
+            dc.capacity = direct.capacity - found;
+            bool used = false;
+            rc = xm_run_jobs(ctx, &job, 1, flags, nullptr, false, stats, nullptr, &dc, &used);
+            if (rc != XM_OK) break;
+            if (!used) {   // this chunk's matches did not fit: redo the whole match into device buffers
+                overflow = true;
+                break;
+            }
+            found += ctx->h_counters[0];
+        }
+        if (rc == XM_OK && overflow) {
+            cudaStreamSynchronize(s2);
+            rc = crossmatch_whole(ctx, A, nA, sb, sr_deg, zh_deg, flags, out, stats);
+        } else if (rc == XM_OK) {
+            out->count = found;
+            ctx->res.count = 0;   // nothing left on the device for xm_fetch_pairs
+            if (stats) stats->n_match = found;
+        }
+    }
+    cudaStreamSynchronize(s2);
+    xm_segment_free(sa);
+    xm_segment_free(sb);
+    if (rc == XM_OK && stats) {
+        XM_CUDA(ctx, cudaEventRecord(ctx->ev[7], st));
+        XM_CUDA(ctx, cudaEventSynchronize(ctx->ev[7]));
+        cudaEventElapsedTime(&stats->ms_total, ctx->ev[6], ctx->ev[7]);
+    }
     return rc;
 }
 

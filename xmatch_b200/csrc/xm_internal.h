@@ -72,8 +72,13 @@ struct xm_ctx {
     size_t d_plans_bytes = 0;
     uint32_t *h_tiles = nullptr; // pinned: tile totals read back after the count pass
     void *build_tmp = nullptr;   // zone-build scratch, shared by the context's builds
-    void *stage = nullptr;       // host records copied here by xm_segment_build
+    void *stage = nullptr;       // host records copied here by xm_segment_build (and A of xm_crossmatch)
     size_t stage_bytes = 0;
+    void *stage2 = nullptr;      // B of xm_crossmatch
+    size_t stage2_bytes = 0;
+    cudaStream_t stream2 = nullptr;   // copies that overlap work on stream
+    cudaEvent_t ev_b2 = nullptr;
+    cudaEvent_t ev_slot[2] = {nullptr, nullptr};   // xm_crossmatch: a chunk of A has landed in a staging slot
     size_t build_tmp_bytes = 0;
     cudaGraphExec_t graph_exec = nullptr;   // the pair-kernel launch sequence (see xm_run_jobs)
     uint64_t graph_launches = 0;
@@ -121,8 +126,12 @@ xm_status xm_seg_storage(xm_segment *seg, uint64_t n);
 xm_status xm_dev_alloc(xm_ctx *ctx, void **p, size_t bytes);
 void xm_dev_free(xm_ctx *ctx, void *p);
 // Runs the pair kernel over the jobs; ctx->res holds the (ungrouped) matches.
+// direct (optional): pinned host buffers (device-accessible pointers) the pair
+// kernel writes the matches into when they hold them all; *direct_used tells
+// whether they did (else the matches are in ctx->res).
 xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags, const xm_tuning *tuning,
-                      bool want_job, xm_stats *stats, float *kernel_ms);
+                      bool want_job, xm_stats *stats, float *kernel_ms, const xm_pairs *direct = nullptr,
+                      bool *direct_used = nullptr);
 // Groups ctx->res by job (res.pairs_g, res.dist_g, res.job_off).
 xm_status xm_group_by_job(xm_ctx *ctx, uint32_t n_jobs, uint32_t *n_launch);
 // Device tables of RA half-widths for each request's zone range (cached).
