@@ -339,9 +339,11 @@ xm_status xm_get_alpha_ranges(xm_ctx *ctx, xm_alpha_req *req, size_t n)
         for (auto &x : th) x.join();
         for (size_t j = 0; j < miss.size(); ++j) {
             xm_alpha_entry e;
-            e.bytes = (off[j + 1] - off[j]) * 8;
+            e.bytes = (off[j + 1] - off[j] + 2) * 8;   // 2 spare entries: the pair kernel copies in 16-byte units
             XM_TRY(xm_dev_alloc(ctx, (void **)&e.dev, e.bytes));
-            XM_CUDA(ctx, cudaMemcpyAsync(e.dev, h.data() + off[j], e.bytes, cudaMemcpyHostToDevice, ctx->stream));
+            XM_CUDA(ctx, cudaMemsetAsync(e.dev, 0, e.bytes, ctx->stream));
+            XM_CUDA(ctx, cudaMemcpyAsync(e.dev, h.data() + off[j], (off[j + 1] - off[j]) * 8, cudaMemcpyHostToDevice,
+                                         ctx->stream));
             ctx->alpha_cache[miss[j]] = e;
             ctx->alpha_bytes += e.bytes;
         }

@@ -41,9 +41,11 @@
 // truncated (Worker.cu:147-148).
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <vector>
 
 #include "xm_internal.h"
+
 #include "xm_match.cuh"
 #include "xm_math.cuh"
 
@@ -504,6 +506,20 @@ __device__ __forceinline__ int a_zone(const uint32_t *__restrict__ a_zoff, int z
     return (__ldg(&a_zoff[lo]) <= i && i < __ldg(&a_zoff[lo + 1])) ? lo : -1;
 }
 
+// Zone of A object i of the staged tile; -1 if the offsets disagree.
+template <class Stage>
+__device__ __forceinline__ int a_zone_s(const Stage &S, uint32_t i)
+{
+    if (S.zf == S.zl) return S.zf;
+    const uint32_t *zo = S.azo_s + S.azo_skew;   // zo[k] = a_zoff[zf + k]
+    int lo = 0, hi = S.zl - S.zf;                // last k with zo[k] <= i
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (zo[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return (zo[lo] <= i && i < zo[lo + 1]) ? S.zf + lo : -1;
+}
+
 // Staged B index -> global B index.
 __device__ __forceinline__ uint32_t staged_global(const BView &V, int nseg, uint32_t q)
 {
@@ -853,7 +869,16 @@ struct StageT {
     uint32_t job, b_start, b_len, id_skew, zoff_skew, done;
     uint32_t seg_off[kMaxPlanSeg + 1];
     uint32_t seg_g[kMaxPlanSeg];
+    // A's zones of the tile: RA half-widths of [zf, zl] from alpha_s[alpha_skew], zone
+    // offsets of [zf, zl + 1] from azo_s[azo_skew] (copied with the tile)
+    uint32_t alpha_skew, azo_skew;
+    alignas(16) double alpha_s[kZcMax + 2];     // bulk-copy destinations: 16-byte aligned
+    alignas(16) uint32_t azo_s[kZcMax + 8];
 };
+
+static_assert(offsetof(StageT<64>, zoff) % 16 == 0 && offsetof(StageT<128>, zoff) % 16 == 0 &&
+                  offsetof(StageT<256>, zoff) % 16 == 0 && offsetof(StageT<128>, a_id) % 16 == 0,
+              "bulk-copy destinations in a stage are 16-byte aligned");
 
 template <int TILE, int VARIANT, bool COUNT_CAND, bool DIST>
 __global__ void __launch_bounds__(TILE + 32, TILE <= 128 ? 4 : 2)
@@ -894,7 +919,9 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
         const double2 *a_radec = nullptr, *b_radec = nullptr;
         const float4 *a_xyz = nullptr, *b_xyz = nullptr;
         const long long *a_id = nullptr;
-        const uint32_t *b_zoff = nullptr;
+        const uint32_t *b_zoff = nullptr, *a_zoff = nullptr;
+        const double *alpha = nullptr;
+        int alpha_z0 = 0;
         // issue plan words w[16] into the next stage
         auto issue = [&](const uint32_t (&w)[16]) -> bool {
             if (!mbar_wait(&empty[s], phase ^ 1u)) return false;
@@ -908,6 +935,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     const JobDev &J = jobs[job];
                     a_radec = J.a_radec; a_xyz = J.a_xyz; a_id = J.a_id;
                     b_radec = J.b_radec; b_xyz = J.b_xyz; b_zoff = J.b_zoff;
+                    a_zoff = J.a_zoff; alpha = J.alpha; alpha_z0 = J.alpha_z0;
                     cached_job = (int)job;
                 }
                 Stage &S = stages[s];
@@ -926,6 +954,15 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 S.id_skew = a_start - a_even;
                 const uint32_t id_cnt = (a_start + a_len - a_even + 1) & ~1u;
                 uint32_t bytes = a_len * 32u + id_cnt * 8u;
+                // alpha of [zf, zl] and A offsets of [zf, zl + 1], rounded out to 16-byte copies
+                // (alpha tables carry 2 spare entries, zone offsets 8)
+                const uint32_t ae = (uint32_t)(zf - alpha_z0), ae_al = ae & ~1u;
+                S.alpha_skew = ae - ae_al;
+                const uint32_t acnt = (S.alpha_skew + (uint32_t)(zl - zf + 1) + 1u) & ~1u;
+                const uint32_t az_al = (uint32_t)zf & ~3u;
+                S.azo_skew = (uint32_t)zf - az_al;
+                const uint32_t azcnt = (S.azo_skew + (uint32_t)(zl - zf + 2) + 3u) & ~3u;
+                bytes += acnt * 8u + azcnt * 4u;
                 uint32_t zcopy = 0, z_al = 0;
                 if (mode == PLAN_WHOLE) {
                     bytes += b_len * 32u;
@@ -951,6 +988,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 bulk_g2s(S.a_radec, a_radec + a_start, a_len * 16u, &full[s]);
                 bulk_g2s(S.a_xyz, a_xyz + a_start, a_len * 16u, &full[s]);
                 bulk_g2s(S.a_id, a_id + a_even, id_cnt * 8u, &full[s]);
+                bulk_g2s(S.alpha_s, alpha + ae_al, acnt * 8u, &full[s]);
+                bulk_g2s(S.azo_s, a_zoff + az_al, azcnt * 4u, &full[s]);
                 if (mode == PLAN_WHOLE) {
                     if (b_len) {
                         bulk_g2s(S.b_radec, b_radec + b_start, b_len * 16u, &full[s]);
@@ -1061,13 +1100,13 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 a.ra = ra.x;
                 a.dec = ra.y;
                 a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
-                a.zone = a_zone(J.a_zoff, S.zf, S.zl, S.a_start + t);
-                if (a.zone < J.alpha_z0 || a.zone > J.z_hi) {   // outside the job's zones and its alpha table
+                a.zone = a_zone_s(S, S.a_start + t);
+                if (a.zone < 0) {   // offsets disagree: never for a consistent segment
                     atomicExch(&out.counters[7], 1ull);
                     a.zone = 0;
                     a.alpha = -1.0;   // empty windows, no candidates
                 } else {
-                    a.alpha = __ldg(&J.alpha[a.zone - J.alpha_z0]);
+                    a.alpha = S.alpha_s[S.alpha_skew + (a.zone - S.zf)];
                 }
                 a.full_ring = a.alpha >= 3.0;
                 a.id = S.a_id[S.id_skew + t];
@@ -1102,13 +1141,13 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 const double2 rd = S.a_radec[t];
                 ra_a = rd.x;
                 dec_a = rd.y;
-                za = a_zone(J.a_zoff, S.zf, S.zl, S.a_start + t);
-                if (za < J.alpha_z0 || za > J.z_hi) {
+                za = a_zone_s(S, S.a_start + t);
+                if (za < 0) {
                     atomicExch(&out.counters[7], 1ull);
                     za = 0;
                     alpha = -1.0;
                 } else {
-                    alpha = __ldg(&J.alpha[za - J.alpha_z0]);
+                    alpha = S.alpha_s[S.alpha_skew + (za - S.zf)];
                 }
                 const Win wn = make_win(ra_a, alpha, K.raq_shift);
                 n = lane_ranges(V, K, wn, alpha >= 3.0, za, L.r[lane], nr);
