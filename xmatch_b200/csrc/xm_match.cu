@@ -14,7 +14,9 @@
 //   UNION   (a single-zone tile whose band is too large) per B zone only the
 //           union of the tile's RA windows, [ra_first - alpha, ra_last +
 //           alpha], when no RA-wraparound window can be non-empty;
-//   GLOBAL  neither fits: the windows are bisected in global memory.
+//   pieces  a band too large for one stage, cut along B into consecutive
+//           ranges that are each staged as a WHOLE plan (see tile_pieces);
+//   GLOBAL  none of these fits: the windows are bisected in global memory.
 //
 // Pair kernel.  Warp-specialised and persistent: warp 0 claims tiles from a
 // global counter (`chunk` at a time) and streams each tile's A objects and
@@ -229,6 +231,24 @@ __device__ __forceinline__ uint32_t upper_v(const BView &V, uint32_t lo, uint32_
         if (raq_at(V.xyz, mid) <= t) lo = mid + 1; else hi = mid;
     }
     return lo;
+}
+
+// First k in [lo, end) with raq[k] > t, by galloping from lo: a window holds
+// few objects, so the common answers (lo, lo + 1) take one or two loads.
+__device__ __forceinline__ uint32_t upper_gallop(const BView &V, uint32_t lo, uint32_t end, uint32_t t)
+{
+    uint32_t step = 1, b;
+    for (;;) {                     // every k in [lo_start, lo) has raq[k] <= t
+        b = lo + step - 1;
+        if (b >= end) {
+            b = end;
+            break;
+        }
+        if (raq_at(V.xyz, b) > t) break;   // answer in [lo, b]
+        lo = b + 1;
+        step <<= 1;
+    }
+    return upper_v(V, lo, b, t);
 }
 
 __device__ __forceinline__ void open_window(const BView &V, const AObj &a, Cursor &c)
@@ -475,16 +495,16 @@ __device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, 
             XM_PUSH(b0, b1);
         } else {
             const uint32_t j0 = lower_v(V, b0, b1, w.lo);
-            const uint32_t j1 = upper_v(V, j0, b1, w.hi);
+            const uint32_t j1 = upper_gallop(V, j0, b1, w.hi);
             XM_PUSH(j0, j1);
             if (w.lo2 <= w.hi2 && w.hi2 >= raq_at(V.xyz, b0)) {
                 const uint32_t w0 = lower_v(V, b0, j0, w.lo2);
-                const uint32_t w1 = upper_v(V, w0, j0, w.hi2);
+                const uint32_t w1 = upper_gallop(V, w0, j0, w.hi2);
                 XM_PUSH(w0, w1);
             }
             if (w.lo3 <= w.hi3 && w.lo3 <= raq_at(V.xyz, b1 - 1)) {
                 const uint32_t w0 = lower_v(V, j1, b1, w.lo3);
-                const uint32_t w1 = upper_v(V, w0, b1, w.hi3);
+                const uint32_t w1 = upper_gallop(V, w0, b1, w.hi3);
                 XM_PUSH(w0, w1);
             }
         }
@@ -691,31 +711,51 @@ __device__ __forceinline__ void for_each_tile(const JobDev &J, const ZoneView &V
     }
 }
 
-// A tile whose zones have no RA cut (alpha >= 3, near the poles) tests its
-// whole B band.  When that is many pairs it is split along B into pieces of
-// at most cap_b objects, each staged and tested as its own plan; pieces go
-// to the "heavy" queue that the pair kernel hands out first, one at a time.
-// Returns the number of pieces (1 = not split) and the piece size.
+// Tiles whose B band does not fit one stage are split along B into pieces,
+// each staged and tested as its own WHOLE plan over a consecutive B range
+// (the pair kernel clips every zone's window to the piece):
+//  - a tile whose zones have no RA cut (alpha >= 3, near the poles) tests its
+//    whole band; when that is many pairs it is cut into pieces of at most
+//    cap_b objects that go to the "heavy" queue the pair kernel hands out
+//    first, one at a time;
+//  - a tile whose objects cover the whole RA ring (several packed zones, or
+//    one whole small zone) has no narrower union of windows to stage; when
+//    its band holds more than cap_b objects it is cut into at most
+//    kMaxSplit near-equal normal pieces (beyond that, the global cursor).
+// Returns the number of pieces (1 = not split), the piece size and the queue.
+constexpr uint32_t kMaxSplit = 8;
+
 __device__ __forceinline__ uint32_t tile_pieces(const JobDev &J, const ZoneView &V, uint32_t len, int zf, int zl,
-                                                uint32_t cap_b, uint32_t *piece)
+                                                uint32_t tile, uint32_t cap_b, uint32_t *piece, bool *heavy)
 {
     const int band_lo = max(0, zf - J.nz), band_hi = min(J.n_zones - 1, zl + J.nz);
     const uint32_t nseg = (uint32_t)(band_hi - band_lo + 1);
     const uint32_t b_len = V.b(band_hi + 1) - V.b(band_lo);
     *piece = b_len;
+    *heavy = false;
+    if ((int)nseg > kMaxBand) return 1;
     const bool full_ring = V.alpha(zf) >= 3.0 || V.alpha(zl) >= 3.0;
-    if (!full_ring || (int)nseg > kMaxBand || (uint64_t)len * b_len <= kHeavyPairs) return 1;
-    uint32_t pc = max(32u, kHeavyPairs / max(len, 1u));
-    pc = min(pc, cap_b);
-    uint32_t n = (b_len + pc - 1) / pc;
-    if (n > kMaxPieces) {
-        pc = (b_len + kMaxPieces - 1) / kMaxPieces;
-        if (pc > cap_b) return 1;
-        n = (b_len + pc - 1) / pc;   // every piece starts inside the band
+    if (full_ring && (uint64_t)len * b_len > kHeavyPairs) {
+        uint32_t pc = max(32u, kHeavyPairs / max(len, 1u));
+        pc = min(pc, cap_b);
+        uint32_t n = (b_len + pc - 1) / pc;
+        if (n > kMaxPieces) {
+            pc = (b_len + kMaxPieces - 1) / kMaxPieces;
+            if (pc > cap_b) return 1;
+            n = (b_len + pc - 1) / pc;   // every piece starts inside the band
+        }
+        if (n <= 1) return 1;
+        *piece = pc;
+        *heavy = true;
+        return n;
     }
-    if (n <= 1) return 1;
-    *piece = pc;
-    return n;
+    if (b_len > cap_b && (zf != zl || 2 * len <= tile)) {
+        const uint32_t n = (b_len + cap_b - 1) / cap_b;
+        if (n > kMaxSplit) return 1;
+        *piece = (b_len + n - 1) / n;
+        return n;
+    }
+    return 1;
 }
 
 // Tiles per work item: cnt[item] normal plans, cnt[n_items + item] heavy pieces.
@@ -729,8 +769,9 @@ __global__ void tiles_count(const JobDev *__restrict__ jobs, int n_jobs, uint32_
     const ZoneView V = global_view(J);
     for_each_tile(J, V, item, zc, tile, [&](uint32_t, uint32_t len, int zf, int zl) {
         uint32_t piece;
-        const uint32_t n = tile_pieces(J, V, len, zf, zl, cap_b, &piece);
-        if (n > 1) h += n; else ++c;
+        bool heavy;
+        const uint32_t n = tile_pieces(J, V, len, zf, zl, tile, cap_b, &piece, &heavy);
+        if (heavy) h += n; else c += n;
     });
     cnt[item] = c;
     cnt[n_items + item] = h;
@@ -790,18 +831,20 @@ tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32
         for (int k = 0; k < kMaxPlanSeg; ++k) P.seg_g[k] = P.seg_len[k] = 0;
         const uint32_t zword = (min(nseg, 255u) << 8) | ((uint32_t)(zl - zf) << 16);
         uint32_t piece;
-        const uint32_t npc = tile_pieces(J, V, len, zf, zl, cap_b, &piece);
+        bool heavy;
+        const uint32_t npc = tile_pieces(J, V, len, zf, zl, tile, cap_b, &piece, &heavy);
         if (npc > 1) {
-            // heavy: WHOLE plans over consecutive B pieces of the band, one per lane
+            // WHOLE plans over consecutive B pieces of the band, one per lane
             P.mode = PLAN_WHOLE | zword;
+            uint32_t &dst = heavy ? oh : o;
             for (uint32_t q = lane; q < npc; q += 32) {
                 TilePlan Q = P;
                 Q.b_start = B0 + q * piece;
                 Q.b_len = min(piece, B1 - Q.b_start);
-                if (oh + q < max_tiles) store_plan(plans + oh + q, Q);
+                if (dst + q < max_tiles) store_plan(plans + dst + q, Q);
                 else atomicExch(err, 1ull);
             }
-            oh += npc;
+            dst += npc;
             return;
         }
         uint32_t mode = PLAN_GLOBAL;
@@ -1167,7 +1210,6 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     a.full_ring = alpha >= 3.0;
                     a.id = S.a_id[S.id_skew + t];
                     a.gi = S.a_start + t;
-                a.gi = S.a_start + t;
                     a.have_xyz = false;
                     test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
                 }
