@@ -77,8 +77,20 @@ static float round_down_f(double v)
 // chord^2 is below T then ||D|| < sqrt(T)(1 + 8u64) = R, and the FP32 value,
 // with one rounding of each difference and three in the fused sum of squares,
 // is at most H = ((R + delta)(1 + u32))^2 (1 + u32)^3.  A pair whose FP32
-// value exceeds H therefore cannot match; thr_lo is the mirror bound below
-// which the FP64 value is certainly under T (used for statistics only).
+// value exceeds H therefore cannot match.
+//
+// thr_lo is the mirror bound: an FP32 value below it implies ||D|| < sqrt(T)
+// (1 - eta) with eta = 2^-20, so the FP64 chord^2 is under T and the angular
+// distance theta of the two (FP64) positions is below r (1 - eta) up to a few
+// units of 1e-16.  Such a pair also passes the reference's two cuts whenever
+// the A zone has an RA cut (alpha < 3 rad, i.e. not the 180-degree sentinel):
+// |dec_a - dec_b| <= theta < r, and the RA offset of a point within theta is at
+// most the exact half-width of a cap of radius theta at |dec_a|, which is below
+// the zone's alpha (computed for radius r at the zone's largest |dec| plus
+// 0.01 r, and never below the exact half-width) by at least (r - theta).  Both
+// margins, about r eta, dwarf the FP64 rounding of the cut arithmetic (below
+// 64 u64 2 pi) once r eta exceeds that; for smaller radii thr_lo is 0 and every
+// pair under thr_hi is decided by the full FP64 predicate.
 xm_status xm_make_params(double sr_deg, double zh_deg, xm_match_params *p)
 {
     if (!(sr_deg > 0) || !(zh_deg > 0) || !std::isfinite(sr_deg) || !std::isfinite(zh_deg)) return XM_ERR_INVALID;
@@ -94,9 +106,10 @@ xm_status xm_make_params(double sr_deg, double zh_deg, xm_match_params *p)
     double H = (R + delta) * (1 + u32);
     H = H * H * std::pow(1 + u32, 3) * (1 + 1e-6);
     p->thr_hi = round_up_f(H);
-    double Rl = rt * (1 - 8 * u64) - delta;
+    const double eta = std::ldexp(1.0, -20);
+    double Rl = rt * (1 - eta) - delta;
     double L = 0;
-    if (Rl > 0) {
+    if (Rl > 0 && p->sr_rad * eta > 64 * u64 * XM_TWO_PI) {
         L = Rl * (1 - u32);
         L = L * L * std::pow(1 - u32, 3) * (1 - 1e-6);
     }

@@ -152,7 +152,7 @@ void xm_raq_layout(int32_t n_zones, int *raq_bits, int *passes);
 struct xm_match_params {
     double sr_deg, sr_rad, sr_dist2;
     float thr_hi;       // FP32 reject threshold: c32 > thr_hi => chord^2 >= sr_dist2
-    float thr_lo;       // c32 < thr_lo => chord^2 < sr_dist2 (statistics only)
+    float thr_lo;       // c32 < thr_lo => chord^2 < sr_dist2 and, with alpha < 3, both cuts hold
     int32_t nz;
 };
 xm_status xm_make_params(double sr_deg, double zh_deg, xm_match_params *p);

@@ -194,7 +194,6 @@ struct AObj {
 //   UNION  (staged): band zone k -> [off[k], off[k+1]), global g[k] + (q - off[k]);
 //   global: zone zb -> [zoff[zb], zoff[zb+1]) of the segment itself.
 struct BView {
-    const double2 *radec;
     const float4 *xyz;
     bool staged, whole;
     int band_lo;
@@ -354,7 +353,6 @@ __device__ __forceinline__ int find_job(const JobDev *__restrict__ jobs, int n_j
     return lo;
 }
 
-constexpr int kStages = 2;
 constexpr int kWarpBuf = 32;
 
 constexpr int kMaxRanges = 9;   // 3 windows x up to 3 zones per lane; beyond that the cursor path
@@ -462,6 +460,77 @@ __device__ __forceinline__ bool cuts_k(const JobScalars &K, double ra_a, double 
     return fabs(d) < alpha || fabs(__dsub_rn(d, XM_TWO_PI)) < alpha || fabs(__dadd_rn(d, XM_TWO_PI)) < alpha;
 }
 
+// Staged index range of band zone zb (clipped to the staged piece for WHOLE).
+__device__ __forceinline__ void zone_range(const BView &V, int zb, uint32_t &b0, uint32_t &b1)
+{
+    const int k = zb - V.band_lo;
+    if (V.whole) {
+        b0 = min(max(V.zoff[k], V.base), V.base + V.len) - V.base;
+        b1 = min(max(V.zoff[k + 1], V.base), V.base + V.len) - V.base;
+    } else {
+        b0 = V.off[k];
+        b1 = V.off[k + 1];
+    }
+}
+
+// lane_ranges for at most three B zones with an RA cut (nz = 1): the three
+// direct-window bisections run interleaved, one step of each per iteration,
+// so that their shared-memory loads overlap; the upper ends are galloped.
+__device__ __forceinline__ int lane_ranges3(const BView &V, const Win &w, int zlo, int zhi, uint32_t *rr, int &nr)
+{
+    uint32_t b0[3], b1[3], lo[3], hi[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        b0[k] = b1[k] = 0;
+        if (zlo + k <= zhi) zone_range(V, zlo + k, b0[k], b1[k]);
+        lo[k] = b0[k];
+        hi[k] = b1[k];
+    }
+    // first k in [b0, b1) with raq >= w.lo, per zone
+    while (lo[0] < hi[0] || lo[1] < hi[1] || lo[2] < hi[2]) {
+        uint32_t v[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) v[k] = raq_at(V.xyz, lo[k] < hi[k] ? (lo[k] + hi[k]) >> 1 : 0u);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (lo[k] < hi[k]) {
+                const uint32_t mid = (lo[k] + hi[k]) >> 1;
+                if (v[k] < w.lo) lo[k] = mid + 1; else hi[k] = mid;
+            }
+        }
+    }
+    int total = 0;
+    nr = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const uint32_t j0 = lo[k];
+        uint32_t j1 = j0;
+        if (j0 < b1[k] && raq_at(V.xyz, j0) <= w.hi) j1 = upper_gallop(V, j0 + 1, b1[k], w.hi);
+        if (j1 > j0) {
+            rr[nr++] = j0 | ((j1 - j0) << 16);
+            total += (int)(j1 - j0);
+        }
+        if (b0[k] >= b1[k]) continue;
+        if (w.lo2 <= w.hi2 && w.hi2 >= raq_at(V.xyz, b0[k])) {
+            const uint32_t w0 = lower_v(V, b0[k], j0, w.lo2);
+            const uint32_t w1 = upper_gallop(V, w0, j0, w.hi2);
+            if (w1 > w0) {
+                rr[nr++] = w0 | ((w1 - w0) << 16);
+                total += (int)(w1 - w0);
+            }
+        }
+        if (w.lo3 <= w.hi3 && w.lo3 <= raq_at(V.xyz, b1[k] - 1)) {
+            const uint32_t w0 = lower_v(V, j1, b1[k], w.lo3);
+            const uint32_t w1 = upper_gallop(V, w0, b1[k], w.hi3);
+            if (w1 > w0) {
+                rr[nr++] = w0 | ((w1 - w0) << 16);
+                total += (int)(w1 - w0);
+            }
+        }
+    }
+    return total;
+}
+
 // Phase 1: a lane's candidate ranges in the staged view (same sets as the
 // cursor enumeration of next_candidate).  Returns the number of candidates,
 // or -1 if the ranges do not fit the per-lane list.
@@ -471,6 +540,7 @@ __device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, 
     nr = 0;
     int total = 0;
     const int zlo = max(0, zone - K.nz), zhi = min(K.n_zones - 1, zone + K.nz);
+    if (!full_ring && zhi - zlo <= 2) return lane_ranges3(V, w, zlo, zhi, rr, nr);
     for (int zb = zlo; zb <= zhi; ++zb) {
         uint32_t b0, b1;
         const int k = zb - V.band_lo;
@@ -568,7 +638,7 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
         cn.tested++;
         bool m = false;
         double c2 = 0;
-        const double2 rb = V.radec[q];
+        const double2 rb = __ldg(&J.b_radec[global_index(V, c.zb, q)]);
         if (VARIANT == 0) {   // FP32 reject above thr_hi, accept below thr_lo, FP64 decision between
             if (COUNT_CAND) cn.cand += cuts_pass(J, a, rb) ? 1ull : 0ull;
             const float4 fb = V.xyz[q];
@@ -897,10 +967,14 @@ tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32
 // Warp-specialised pair kernel: warp 0 produces (bulk copies into a ring of
 // stages), warps 1..C consume (one A object per thread).
 // ---------------------------------------------------------------------------
-template <int TILE>
+// B's ra/dec are staged only for the all-FP64 variant (RADEC), which cuts every
+// candidate; the FP32 filter reads them from global memory for the few pairs
+// inside its margin band.  Without them a stage is small enough for three.
+template <int TILE, bool RADEC>
 struct StageT {
     static constexpr int kCapB = 4 * TILE;
-    double2 b_radec[kCapB];
+    static constexpr int kStages = RADEC ? 2 : 3;
+    double2 b_radec[RADEC ? kCapB : 1];
     float4 b_xyz[kCapB];
     double2 a_radec[TILE];
     float4 a_xyz[TILE];
@@ -919,8 +993,15 @@ struct StageT {
     alignas(16) uint32_t azo_s[kZcMax + 8];
 };
 
-static_assert(offsetof(StageT<64>, zoff) % 16 == 0 && offsetof(StageT<128>, zoff) % 16 == 0 &&
-                  offsetof(StageT<256>, zoff) % 16 == 0 && offsetof(StageT<128>, a_id) % 16 == 0,
+template <int TILE, bool RADEC>
+constexpr bool stage_aligned()
+{
+    using S = StageT<TILE, RADEC>;
+    return offsetof(S, zoff) % 16 == 0 && offsetof(S, a_id) % 16 == 0 && offsetof(S, a_radec) % 16 == 0 &&
+           offsetof(S, a_xyz) % 16 == 0 && offsetof(S, b_xyz) % 16 == 0;
+}
+static_assert(stage_aligned<64, false>() && stage_aligned<128, false>() && stage_aligned<256, false>() &&
+                  stage_aligned<64, true>() && stage_aligned<128, true>() && stage_aligned<256, true>(),
               "bulk-copy destinations in a stage are 16-byte aligned");
 
 template <int TILE, int VARIANT, bool COUNT_CAND, bool DIST>
@@ -928,7 +1009,9 @@ __global__ void __launch_bounds__(TILE + 32, TILE <= 128 ? 4 : 2)
 pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans, uint32_t n_heavy,
             uint32_t n_normal, uint32_t chunk, MatchOut out)
 {
-    using Stage = StageT<TILE>;
+    constexpr bool RADEC = VARIANT == 1;
+    using Stage = StageT<TILE, RADEC>;
+    constexpr int kStages = Stage::kStages;
     constexpr int C = TILE / 32;   // consumer warps
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Stage *stages = reinterpret_cast<Stage *>(smem_raw);
@@ -1007,14 +1090,15 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 const uint32_t azcnt = (S.azo_skew + (uint32_t)(zl - zf + 2) + 3u) & ~3u;
                 bytes += acnt * 8u + azcnt * 4u;
                 uint32_t zcopy = 0, z_al = 0;
+                constexpr uint32_t kBBytes = RADEC ? 32u : 16u;   // staged bytes per B object
                 if (mode == PLAN_WHOLE) {
-                    bytes += b_len * 32u;
+                    bytes += b_len * kBBytes;
                     z_al = (uint32_t)band_lo & ~3u;
                     S.zoff_skew = (uint32_t)band_lo - z_al;
                     zcopy = (S.zoff_skew + nseg + 1 + 3) & ~3u;
                     bytes += zcopy * 4u;
                 } else if (mode == PLAN_UNION) {
-                    bytes += b_len * 32u;
+                    bytes += b_len * kBBytes;
                     uint32_t o = 0;
 #pragma unroll
                     for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
@@ -1035,7 +1119,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 bulk_g2s(S.azo_s, a_zoff + az_al, azcnt * 4u, &full[s]);
                 if (mode == PLAN_WHOLE) {
                     if (b_len) {
-                        bulk_g2s(S.b_radec, b_radec + b_start, b_len * 16u, &full[s]);
+                        if (RADEC) bulk_g2s(S.b_radec, b_radec + b_start, b_len * 16u, &full[s]);
                         bulk_g2s(S.b_xyz, b_xyz + b_start, b_len * 16u, &full[s]);
                     }
                     bulk_g2s(S.zoff, b_zoff + z_al, zcopy * 4u, &full[s]);
@@ -1044,7 +1128,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
                         const uint32_t ln = w[12 + q];
                         if (q >= nseg || !ln) continue;
-                        bulk_g2s(S.b_radec + S.seg_off[q], b_radec + w[8 + q], ln * 16u, &full[s]);
+                        if (RADEC) bulk_g2s(S.b_radec + S.seg_off[q], b_radec + w[8 + q], ln * 16u, &full[s]);
                         bulk_g2s(S.b_xyz + S.seg_off[q], b_xyz + w[8 + q], ln * 16u, &full[s]);
                     }
                 }
@@ -1158,7 +1242,6 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 BView V;
                 V.staged = false;
                 V.whole = false;
-                V.radec = J.b_radec;
                 V.xyz = J.b_xyz;
                 V.zoff = J.b_zoff;
                 V.band_lo = 0;
@@ -1169,7 +1252,6 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             V.staged = true;
             V.whole = S.mode == PLAN_WHOLE;
             V.band_lo = S.band_lo;
-            V.radec = S.b_radec;
             V.xyz = S.b_xyz;
             V.zoff = S.zoff + S.zoff_skew;
             V.base = S.b_start;
@@ -1249,25 +1331,36 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                         const uint32_t ta = (warp - 1) * 32u + (uint32_t)owner;
                         cn.tested++;
                         const double2 ra = S.a_radec[ta];
-                        const double2 rb = S.b_radec[q];
                         const double al = L.alpha[owner];
                         double c2 = 0;
+                        uint32_t gq = 0xFFFFFFFFu;   // global index of q, once needed
                         if (VARIANT == 0) {
-                            if (COUNT_CAND) cn.cand += cuts_k(K, ra.x, ra.y, al, rb) ? 1ull : 0ull;
                             const float4 fa = S.a_xyz[ta];
                             const float4 fb = S.b_xyz[q];
                             const float dx = fa.x - fb.x, dy = fa.y - fb.y, dz = fa.z - fb.z;
                             const float c32 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            if (COUNT_CAND) {
+                                gq = staged_global(V, (int)S.nseg, q);
+                                cn.cand += cuts_k(K, ra.x, ra.y, al, __ldg(&J.b_radec[gq])) ? 1ull : 0ull;
+                            }
                             if (!(c32 > K.thr_hi)) {
-                                // below thr_lo the FP64 chord is below the threshold (proven bound):
-                                // FP64 only inside the band, or for the distance
+                                // below thr_lo the FP64 chord is under the threshold and, in a zone
+                                // with an RA cut (alpha < 3), the dec and RA cuts hold (bounds in
+                                // xm_make_params): B's ra/dec and the FP64 vectors are read only
+                                // inside the band, or for the distance
                                 const bool band = c32 >= K.thr_lo;
                                 cn.border += band ? 1ull : 0ull;
-                                if (cuts_k(K, ra.x, ra.y, al, rb)) {
+                                bool pass = true;
+                                if (band || al >= 3.0) {
+                                    if (gq == 0xFFFFFFFFu) gq = staged_global(V, (int)S.nseg, q);
+                                    pass = cuts_k(K, ra.x, ra.y, al, __ldg(&J.b_radec[gq]));
+                                }
+                                if (pass) {
                                     m = true;
                                     if (band || DIST) {
+                                        if (gq == 0xFFFFFFFFu) gq = staged_global(V, (int)S.nseg, q);
                                         const size_t ga = 3 * (size_t)(S.a_start + ta);
-                                        const size_t gb = 3 * (size_t)staged_global(V, (int)S.nseg, q);
+                                        const size_t gb = 3 * (size_t)gq;
                                         c2 = chord2(__ldg(&J.a_xyz64[ga]), __ldg(&J.a_xyz64[ga + 1]),
                                                     __ldg(&J.a_xyz64[ga + 2]), __ldg(&J.b_xyz64[gb]),
                                                     __ldg(&J.b_xyz64[gb + 1]), __ldg(&J.b_xyz64[gb + 2]));
@@ -1279,6 +1372,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                                 }
                             }
                         } else {
+                            const double2 rb = S.b_radec[q];
                             if (cuts_k(K, ra.x, ra.y, al, rb)) {
                                 cn.cand++;
                                 cn.exact++;
@@ -1290,8 +1384,9 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                             }
                         }
                         if (m) {
+                            if (gq == 0xFFFFFFFFu) gq = staged_global(V, (int)S.nseg, q);
                             ida = S.a_id[S.id_skew + ta];
-                            idb = __ldg(&J.b_id[staged_global(V, (int)S.nseg, q)]);
+                            idb = __ldg(&J.b_id[gq]);
                             if (DIST) dist = 2.0 * asin(sqrt(c2) * 0.5);
                         }
                     }
@@ -1325,11 +1420,12 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
     }
 }
 
-template <int TILE>
+template <int TILE, bool RADEC>
 constexpr size_t smem_bytes()
 {
-    return kStages * sizeof(StageT<TILE>) + (TILE / 32) * (sizeof(WBuf) + sizeof(WList)) +
-           2 * kStages * sizeof(uint64_t);
+    using Stage = StageT<TILE, RADEC>;
+    return Stage::kStages * sizeof(Stage) + (TILE / 32) * (sizeof(WBuf) + sizeof(WList)) +
+           2 * Stage::kStages * sizeof(uint64_t);
 }
 
 template <int TILE, int VARIANT, bool CC, bool DIST>
@@ -1337,7 +1433,7 @@ cudaError_t launch_t(const LaunchCfg &L, const JobDev *jobs, const TilePlan *pla
                      uint32_t n_normal, const MatchOut &out, cudaStream_t st)
 {
     auto k = pair_kernel<TILE, VARIANT, CC, DIST>;
-    const size_t smem = smem_bytes<TILE>();
+    const size_t smem = smem_bytes<TILE, VARIANT == 1>();
     static bool attr = false;   // per instantiation
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
