@@ -257,6 +257,11 @@ xm_status xm_unit_vectors(xm_ctx *ctx, const double *ra_deg, const double *dec_d
                           double *xyz);
 /* RA half-width of Common.cu:17-23 for every zone, as the library uses it. */
 xm_status xm_alpha_table(double sr_deg, double zh_deg, double *alpha, int32_t n_zones);
+/* The FP32 chord^2 thresholds XM_FILTER32 uses at radius sr_deg: a pair whose
+ * FP32 chord^2 (from the FP32 unit vectors, fused sum of squares) exceeds
+ * *thr_hi cannot match; one below *thr_lo matches whenever the RA half-width
+ * of A's zone is below 3 rad (0 when the radius is too small for that). */
+xm_status xm_filter_bounds(double sr_deg, float *thr_hi, float *thr_lo);
 
 #ifdef __cplusplus
 }

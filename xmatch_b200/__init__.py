@@ -83,6 +83,13 @@ def alpha_table(sr_deg, zh_deg):
     return out
 
 
+def filter_bounds(sr_deg):
+    """(thr_hi, thr_lo) of the FP32 chord^2 filter at radius sr_deg (float32 values)."""
+    hi, lo = ctypes.c_float(), ctypes.c_float()
+    _check(_lib.xm_filter_bounds(sr_deg, ctypes.byref(hi), ctypes.byref(lo)))
+    return np.float32(hi.value), np.float32(lo.value)
+
+
 class DeviceSegment:
     """A zone-sorted segment resident on the GPU (Segment, Segment.h:22-41)."""
 

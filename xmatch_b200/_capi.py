@@ -113,6 +113,7 @@ SIGNATURES = {
     "xm_segment_build_noalloc": (ctypes.c_int, [ctypes.c_int, P, P, U64, D, P, P, P, P, U64,
                                                 ctypes.POINTER(U64)]),
     "xm_alpha_table": (ctypes.c_int, [D, D, P, I32]),
+    "xm_filter_bounds": (ctypes.c_int, [D, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "xm_crossmatch": (ctypes.c_int, [P, P, U64, P, U64, D, D, U32, ctypes.POINTER(XmPairs), ctypes.POINTER(XmStats)]),
     "xm_serve_open": (ctypes.c_int, [P, P, ctypes.POINTER(XmServeCfg), PP]),
     "xm_serve_submit": (ctypes.c_int, [P, P, U64, D, ctypes.POINTER(U64)]),

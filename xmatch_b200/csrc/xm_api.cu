@@ -1038,3 +1038,14 @@ extern "C" xm_status xm_alpha_table(double sr_deg, double zh_deg, double *alpha,
     xm_host_alpha_table(sr_deg, zh_deg, n_zones, alpha);
     return XM_OK;
 }
+
+extern "C" xm_status xm_filter_bounds(double sr_deg, float *thr_hi, float *thr_lo)
+{
+    if (!thr_hi || !thr_lo) return XM_ERR_INVALID;
+    xm_match_params p;
+    const xm_status s = xm_make_params(sr_deg, 1.0, &p);
+    if (s != XM_OK) return s;
+    *thr_hi = p.thr_hi;
+    *thr_lo = p.thr_lo;
+    return XM_OK;
+}
