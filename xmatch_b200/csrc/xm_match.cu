@@ -360,19 +360,23 @@ constexpr int kMaxRanges = 9;   // 3 windows x up to 3 zones per lane; beyond th
 // Per-warp candidate ranges of phase 1: start | length << 16 (staged indices < 2^16).
 struct WList {
     uint32_t r[32][kMaxRanges];
-    uint32_t pre[32];              // inclusive prefix of candidate counts
+    uint32_t mark[32];             // phase 2: 1 + the lane whose candidates start at this position
     double alpha[32];
 };
 
+// Per-warp match buffer.  An entry holds idA and the ADDRESS of idB in the B
+// segment; the ids are loaded when the buffer is flushed, all lanes at once
+// and under the output atomic, instead of one dependent load per match.
 struct WBuf {
-    longlong2 ab[kWarpBuf];
+    longlong2 ab[kWarpBuf];     // idA, address of idB
     double d[kWarpBuf];
     uint32_t job[kWarpBuf];
     uint32_t count;
 };
 
-// Warp-aggregated append of this iteration's matches to the warp's buffer.
-__device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, long long ida, long long idb,
+// Warp-aggregated append of this iteration's matches to the warp's buffer
+// (pb: address of idB; read here only for entries that overflow the buffer).
+__device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, long long ida, const long long *pb,
                                        double dist, uint32_t job)
 {
     const unsigned act = __activemask();
@@ -390,7 +394,7 @@ __device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, lo
     base = __shfl_sync(bal, base, leader);
     const uint32_t slot = base + rank;
     if (slot < (uint32_t)kWarpBuf) {
-        wb.ab[slot] = make_longlong2(ida, idb);
+        wb.ab[slot] = make_longlong2(ida, (long long)pb);
         wb.d[slot] = dist;
         wb.job[slot] = job;
     }
@@ -402,6 +406,7 @@ __device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, lo
     const int l2 = __ffs(over) - 1;
     unsigned long long g = 0;
     if ((int)lane == l2) g = atomicAdd(&out.counters[0], (unsigned long long)__popc(over));
+    const long long idb = __ldg(pb);
     g = __shfl_sync(over, g, l2);
     g += (unsigned long long)__popc(over & lanemask_lt());
     if (g < out.cap) {
@@ -411,21 +416,30 @@ __device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, lo
     }
 }
 
-// Whole warp (converged): one atomicAdd, then a coalesced copy.
+// Whole warp (converged): one atomicAdd, the idB loads issued under it, then a
+// coalesced copy (entry k by lane k).
 __device__ __forceinline__ void flush_w(WBuf &wb, const MatchOut &out)
 {
+    static_assert(kWarpBuf == 32, "one buffer entry per lane");
     __syncwarp();
     const unsigned lane = threadIdx.x & 31;
     const uint32_t n = wb.count < (uint32_t)kWarpBuf ? wb.count : (uint32_t)kWarpBuf;
     unsigned long long g = 0;
     if (lane == 0 && n) g = atomicAdd(&out.counters[0], (unsigned long long)n);
+    longlong2 e = make_longlong2(0, 0);
+    double d = 0;
+    uint32_t jb = 0;
+    if (lane < n) {
+        e = wb.ab[lane];
+        e.y = __ldg(reinterpret_cast<const long long *>(e.y));
+        if (out.dist) d = wb.d[lane];
+        if (out.job) jb = wb.job[lane];
+    }
     g = __shfl_sync(0xffffffffu, g, 0);
-    for (uint32_t k = lane; k < n; k += 32) {
-        if (g + k < out.cap) {
-            reinterpret_cast<longlong2 *>(out.pairs)[g + k] = wb.ab[k];
-            if (out.dist) out.dist[g + k] = wb.d[k];
-            if (out.job) out.job[g + k] = wb.job[k];
-        }
+    if (lane < n && g + lane < out.cap) {
+        reinterpret_cast<longlong2 *>(out.pairs)[g + lane] = e;
+        if (out.dist) out.dist[g + lane] = d;
+        if (out.job) out.job[g + lane] = jb;
     }
     __syncwarp();
     if (lane == 0) wb.count = 0;
@@ -677,13 +691,13 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
                 m = c2 < J.sr_dist2;
             }
         }
-        long long idb = 0;
+        const long long *pb = nullptr;
         double dist = 0;
         if (m) {
-            idb = __ldg(&J.b_id[global_index(V, c.zb, q)]);
+            pb = &J.b_id[global_index(V, c.zb, q)];
             if (DIST) dist = 2.0 * asin(sqrt(c2) * 0.5);
         }
-        emit_w(wb, out, m, a.id, idb, dist, jx);
+        emit_w(wb, out, m, a.id, pb, dist, jx);
     }
 }
 
@@ -1206,6 +1220,9 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
     // ================= consumers =================
     WBuf &wb = wbufs[warp - 1];
     Counters cn = {0ull, 0ull, 0ull, 0ull};
+    int cur_job = -1;
+    const JobDev *Jp = jobs;
+    JobScalars K = {};
     int s = 0;
     uint32_t phase = 0;
     for (;;) {
@@ -1216,8 +1233,12 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
         Stage &S = stages[s];
         if (S.done) break;
         const uint32_t t = (uint32_t)(warp - 1) * 32u + lane;
-        const JobDev &J = jobs[S.job];
-        const JobScalars K = load_scalars(J);
+        if ((int)S.job != cur_job) {   // job scalars stay in registers while the job does not change
+            cur_job = (int)S.job;
+            Jp = &jobs[cur_job];
+            K = load_scalars(*Jp);
+        }
+        const JobDev &J = *Jp;
         if (S.mode == PLAN_GLOBAL) {
             // band too large to stage: per-lane cursor over global memory
             if (t < S.a_len) {
@@ -1303,24 +1324,34 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
                     if (lane >= (unsigned)o) incl += y;
                 }
-                L.pre[lane] = incl;
+                const uint32_t start = incl - (uint32_t)n;
                 const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-                __syncwarp();
                 // ---- phase 2: the warp walks the flattened candidate list ----
                 for (uint32_t c0 = 0; c0 < total; c0 += 32) {
                     const uint32_t c = c0 + lane;
+                    // owner of candidate c: the last lane with candidates that start at or
+                    // before c -- the lane covering c0 (ballot), or a later lane whose start
+                    // mark lies in (c0, c], found by a max-scan over the marks
+                    const unsigned before = __ballot_sync(0xffffffffu, n > 0 && start <= c0);
+                    L.mark[lane] = 0;
+                    __syncwarp();
+                    if (n > 0 && start > c0 && start < c0 + 32) L.mark[start - c0] = lane + 1;
+                    __syncwarp();
+                    int own = (int)L.mark[lane] - 1;
+                    if (own < 0) own = before ? 31 - __clz(before) : 0;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, own, o);
+                        if (lane >= (unsigned)o) own = max(own, y);
+                    }
+                    const uint32_t own_start = __shfl_sync(0xffffffffu, start, own);
                     bool m = false;
-                    long long ida = 0, idb = 0;
+                    long long ida = 0;
+                    const long long *pb = nullptr;
                     double dist = 0;
                     if (c < total) {
-                        // owner lane: first lane whose inclusive prefix exceeds c
-                        int lo = 0, hi = 31;
-                        while (lo < hi) {
-                            const int mid = (lo + hi) >> 1;
-                            if (L.pre[mid] > c) hi = mid; else lo = mid + 1;
-                        }
-                        const int owner = lo;
-                        uint32_t k = c - (owner ? L.pre[owner - 1] : 0u);
+                        const int owner = own;
+                        uint32_t k = c - own_start;
                         int r = 0;
                         uint32_t rr = L.r[owner][0];
                         while (k >= (rr >> 16)) {
@@ -1386,11 +1417,11 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                         if (m) {
                             if (gq == 0xFFFFFFFFu) gq = staged_global(V, (int)S.nseg, q);
                             ida = S.a_id[S.id_skew + ta];
-                            idb = __ldg(&J.b_id[gq]);
+                            pb = &J.b_id[gq];
                             if (DIST) dist = 2.0 * asin(sqrt(c2) * 0.5);
                         }
                     }
-                    emit_w(wb, out, m, ida, idb, dist, S.job);
+                    emit_w(wb, out, m, ida, pb, dist, S.job);
                     __syncwarp();
                     if (wb.count >= (uint32_t)(kWarpBuf / 2)) flush_w(wb, out);
                 }
