@@ -27,18 +27,23 @@
 // flag that the host reports.
 //
 // Pair test.  Every thread bisects its own windows (direct, and the two
-// wrapped ones for the RA branches of Worker.cu:89,98,110) in the staged ra
-// values and tests each candidate with the reference predicate (Worker.cu:
-// 88-97): dec cut, RA cut, chord^2 < (2 sin(r/2))^2, all FP64 with the unit
-// vectors of the unshifted (ra, dec) -- the branch-3 sign error of
-// Worker.cu:118 fixed.  XM_FILTER32 first evaluates chord^2 in FP32 from the
-// stored FP32 unit vectors and discards a pair only when that value exceeds a
-// bound proven to imply chord^2_FP64 >= threshold; every other pair is
-// decided by the FP64 predicate, so the pair set is the FP64 one bit for bit.
+// wrapped ones for the RA branches of Worker.cu:89,98,110) in the staged
+// quantised ra (raq, xyz.w) of its three B zones; the warp then walks the
+// flattened list of its lanes' candidates.  The reference predicate
+// (Worker.cu:88-97) is: dec cut, RA cut, chord^2 < (2 sin(r/2))^2, all FP64
+// with the unit vectors of the unshifted (ra, dec) -- the branch-3 sign error
+// of Worker.cu:118 fixed.  XM_FILTER32 evaluates chord^2 in FP32 from the
+// FP32 unit vectors first: above thr_hi the pair cannot match; below thr_lo
+// (zones with an RA cut) it matches and the cuts provably hold; in between,
+// and in full-ring zones, B's ra/dec and both FP64 unit vectors are read and
+// the FP64 predicate decides.  The bounds are derived in xm_make_params, so
+// the pair set is the FP64 one bit for bit.  XM_PLAIN64 applies the FP64
+// predicate with per-pair sincos to every candidate.
 //
 // Output.  Matches are compacted per warp with __ballot_sync/__popc into the
-// warp's buffer in shared memory, which is appended to global memory with
-// one atomicAdd per flush (Worker.cu:128-240 uses two Hillis-Steele scans per
+// warp's buffer in shared memory (idA and the address of idB), which is
+// appended to global memory with one atomicAdd per flush, the idB loads
+// issued under it (Worker.cu:128-240 uses two Hillis-Steele scans per
 // block).  A full output buffer is detected and reported, never silently
 // truncated (Worker.cu:147-148).
 #include <algorithm>
