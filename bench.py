@@ -675,16 +675,23 @@ def run_c4(args):
         queries.append((q, qr.uniform(0.5, 10.0) * ARCSEC))
     arrivals = np.cumsum(qr.exponential(1.0 / args.c4_rate, len(queries)))
     srv = xm.Server(ctx, cat)
-    # warm-up before the clock (memory pools, graph, result buffers): a few
-    # queries of the same distribution, not part of the measured stream
+    # warm-up before the clock (memory pools, graph, result buffers): queries of
+    # the same distribution, not part of the measured stream; 4 one at a time,
+    # then 8 in a burst so that multi-query batches (matches grouped by query)
+    # have run too
     wr = np.random.default_rng(3004)
-    for k in range(8):
+    warm = []
+    for k in range(12):
         n = int(np.exp(wr.uniform(np.log(100), np.log(1_000_000))))
         ra_q, dec_q = cap_points(wr, n, wr.uniform(0, 360), np.degrees(np.arcsin(wr.uniform(-1, 1))),
                                  wr.uniform(0.05, 5.0))
         q = np.empty(n, xm.OBJ_DTYPE)
         q["id"], q["ra"], q["dec"] = np.arange(n), ra_q, dec_q
-        srv.poll(srv.submit(q, wr.uniform(0.5, 10.0) * ARCSEC))
+        warm.append((q, wr.uniform(0.5, 10.0) * ARCSEC))
+    for q, r in warm[:4]:
+        srv.poll(srv.submit(q, r))
+    for t in [srv.submit(q, r) for q, r in warm[4:]]:
+        srv.poll(t)
     tickets = [None] * len(queries)
     ready = threading.Event()
 
