@@ -55,7 +55,6 @@ def parse():
     ap.add_argument("--dec-band", type=float, nargs=2, default=None, metavar=("LO", "HI"),
                     help="keep only sources with dec in [LO, HI) deg (same density, smaller case for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
     ap.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
                     help="c1: 50Mx50M crossmatch (the headline); c2: 4,096-job batch; c3: precision stress; "
@@ -71,9 +70,21 @@ def parse():
     return ap.parse_args()
 
 
+def _load_by_path(name):
+    """A module of xmatch_b200 that needs neither the package nor its CUDA
+    library (synth, pairhash), loaded from its file: the reference arm must not
+    load this project's library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("xm_" + name, os.path.join(ROOT, "xmatch_b200", name + ".py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def load_workload(n, seed=1001):
     """config1 catalogs, cached per box under /tmp (generation takes ~30 s at 50M)."""
-    from xmatch_b200 import OBJ_DTYPE, synth
+    synth = _load_by_path("synth")
+    OBJ_DTYPE = synth.OBJ_DTYPE
     cache = "/tmp/xmatch_b200_cfg1_%d_%d" % (n, seed)
     fa, fb = cache + "_A.bin", cache + "_B.bin"
     if os.path.exists(fa) and os.path.exists(fb):
@@ -152,32 +163,35 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def cpu_baseline(A, B, r_deg, target_s, steps=1):
+# The CPU sample of the workload, the same in both arms: A's sources in a dec
+# band of the sky and B's within 2r of it (every match of those A sources),
+# about 17 % of the 50M catalogs and a few seconds of work per run on 16 cores.
+CPU_SAMPLE_DEC = (0.0, 10.0)
+
+
+def cpu_sample(A, B, r_deg):
+    lo, hi = CPU_SAMPLE_DEC
+    a = A[(A["dec"] >= lo) & (A["dec"] < hi)]
+    b = B[(B["dec"] >= lo - 2 * r_deg) & (B["dec"] < hi + 2 * r_deg)]
+    return a, b
+
+
+def cpu_baseline(A, B, r_deg, steps=1):
     """The reference algorithm (zone-pair loop, all pairs per zone pair, per-pair
     FP64 sincos; Worker.cu:82-123,330-366) restated in C (oracle/), on all
-    host cores, over a dec band of the same catalogs sized to ~target_s."""
+    host cores, over the fixed dec-band sample of the same catalogs."""
     import oracle
     cores = os.cpu_count() or 1
-    lo = 0.0
-    width = 0.05
-    while True:
-        a = A[(A["dec"] >= lo) & (A["dec"] < lo + width)]
-        b = B[(B["dec"] >= lo - 2 * r_deg) & (B["dec"] < lo + width + 2 * r_deg)]
+    a, b = cpu_sample(A, B, r_deg)
+    times = []
+    for _ in range(steps):
         t0 = time.perf_counter()
         p, _, st = oracle.xmatch(a, b, r_deg, mode=oracle.MODE_ALLPAIRS_SINCOS, nthreads=cores, with_dist=True)
-        dt = time.perf_counter() - t0
-        if dt * 4 >= target_s or width >= 20:
-            break
-        width = min(20.0, width * max(2.0, min(8.0, target_s / max(dt, 1e-3) / 2)))
-    times = [dt]
-    for _ in range(steps - 1):
-        t0 = time.perf_counter()
-        oracle.xmatch(a, b, r_deg, mode=oracle.MODE_ALLPAIRS_SINCOS, nthreads=cores, with_dist=True)
         times.append(time.perf_counter() - t0)
     t = min(times)
     return {"value": st.n_cand / t, "unit": UNIT, "cores": cores, "kind": "port",
             "seconds": t, "sample": "A sources with dec in [%g, %g) deg (%d) x B within +-2r (%d): %d candidate "
-            "pairs, %d matches; includes the CPU zone sort" % (lo, lo + width, len(a), len(b), st.n_cand, len(p)),
+            "pairs, %d matches; includes the CPU zone sort" % (CPU_SAMPLE_DEC + (len(a), len(b), st.n_cand, len(p))),
             "matches": len(p)}
 
 
@@ -209,12 +223,9 @@ def run_reference(args):
         return 0
     A, B = load_workload(args.n)
     r = 1.0 * ARCSEC
-    cb = cpu_baseline(A, B, r, max(2.0, args.cpu_seconds / 4))
-    # fixed sample, W untimed + K timed steps
+    # the fixed sample of the GPU arm's cpu_baseline, W untimed + K timed steps
     import oracle
-    lo, hi = [float(x) for x in cb["sample"].split("[")[1].split(")")[0].split(",")]
-    a = A[(A["dec"] >= lo) & (A["dec"] < hi)]
-    b = B[(B["dec"] >= lo - 2 * r) & (B["dec"] < hi + 2 * r)]
+    a, b = cpu_sample(A, B, r)
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
         oracle.xmatch(a, b, r, mode=oracle.MODE_ALLPAIRS_SINCOS, nthreads=cores)
@@ -223,12 +234,14 @@ def run_reference(args):
         p, _, st = oracle.xmatch(a, b, r, mode=oracle.MODE_ALLPAIRS_SINCOS, nthreads=cores)
     dt = (time.perf_counter() - t0) / args.steps
     v = st.n_cand / dt
+    sample = ("A sources with dec in [%g, %g) deg (%d) x B within +-2r (%d): %d candidate pairs, %d matches; "
+              "includes the CPU zone sort" % (CPU_SAMPLE_DEC + (len(a), len(b), st.n_cand, len(p))))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config1 mixture)",
             "config": {"workload": "config1 50Mx50M r=zh=1\" (CPU sample: dec band)", "n_per_catalog": args.n,
-                       "r_arcsec": 1.0, "zh_arcsec": 1.0, "sample": cb["sample"]},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": cb["sample"]},
+                       "r_arcsec": 1.0, "zh_arcsec": 1.0, "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference has no CPU implementation of the path; this is the oracle's restatement of "
                     "its algorithm (zone-pair loop, all pairs per zone pair, per-pair sincos), all host threads"}
@@ -250,9 +263,11 @@ def reference_gpu_kernel(A, B, r, cores):
     except ImportError:
         return {"unavailable": "torch missing"}
     secs, launches, appended = ref_kernel.time_zone_loop(A, B, r)
-    _, _, st = oracle.xmatch(A, B, r, nthreads=cores, with_dist=False)
+    p, _, st = oracle.xmatch(A, B, r, nthreads=cores, with_dist=False)
+    digest = _load_by_path("pairhash").pairset_digest(p)
     return {"value": st.n_cand / secs, "unit": UNIT, "seconds": secs, "launches": launches,
-            "pairs_appended": appended, "matches_oracle": st.n_match,
+            "pairs_appended": appended, "matches_oracle": st.n_match, "candidates_oracle": st.n_cand,
+            "oracle_pair_set_digest": digest,
             "what": "one launch per zone pair, 16x16 blocks, FP64 with sincos per pair (Worker.cu:66-240,330-366)"}
 
 
@@ -348,8 +363,7 @@ def run_ours(args):
     dom = max(per, key=per.get)
     # DRAM bytes (read + write) per launch from ncu captures of the same kernels on the config-1 catalogs
     # cut to a dec band (same objects per zone), scaled by the objects a launch processes: the zone build
-    # and plan kernels on dec 0..10 deg (profiles/build_and_pair_kernels_config1_band.md), the pair kernel
-    # on dec 30..60 deg (profiles/pair_kernel_config1_band30_60.md)
+    # and plan kernels on dec 0..10 deg, the pair kernel on dec 30..60 deg
     band_a = 4_397_838
     band_a_pair = 8_919_127
     traffic_per_obj = {"pair_kernel": (586.95e6 + 90.34e6) / band_a_pair,
@@ -368,6 +382,58 @@ def run_ours(args):
     pipeline = {"alg_bytes": pipeline_bytes, "GB/s": pipeline_bytes / (ms * 1e-3) / 1e9,
                 "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / hbm}
     value = whole_job_rate(world, n_cand, ms)
+    # FP32 issue rate of the pair loop: 7 FP32-pipe instructions per tested pair
+    # (3 FSUB, 1 FMUL, 2 FFMA, 1 compare) against 128 FP32 lanes per SM at the
+    # SM clock sampled during the timed steps
+    sm_count = ctx.info()["sm_count"]
+    f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    tested = stats.n_tested / K
+    fp32_ach = tested * 7 / (per["pair_kernel"] * 1e-3) if per["pair_kernel"] > 0 else 0.0
+    fp32_issue = {"tested_pairs": int(tested), "instr_per_pair": 7, "achieved_lane_instr_per_s": fp32_ach,
+                  "peak_lane_instr_per_s": sm_count * 128 * f_sm, "frac": fp32_ach / (sm_count * 128 * f_sm),
+                  "sm_mhz": f_sm / 1e6, "kernel": "pair_kernel"}
+
+    # ---- the headline step's pair set against the oracle's (untimed) ----
+    pairhash = _load_by_path("pairhash")
+    pairs_dev, _ = ctx.fetch(n_match, with_dist=False)
+    pair_set = {"digest": pairhash.pairset_digest(pairs_dev)}
+    del pairs_dev
+    gold = os.path.join(ROOT, "tests", "golden", "config1_pairset.json")
+    if os.path.exists(gold) and not args.dec_band:
+        with open(gold) as f:
+            g = json.load(f)
+        if (g["n"] == n and pairhash.inputs_fingerprint(A) == g["inputs"]["A"]
+                and pairhash.inputs_fingerprint(B) == g["inputs"]["B"]):
+            pair_set.update({"oracle_digest": g["digest"], "oracle_candidates": g["candidates"],
+                             "equal_to_oracle": pair_set["digest"] == g["digest"] and n_cand == g["candidates"],
+                             "oracle_source": "tests/golden/config1_pairset.json (oracle on the same seeded "
+                                              "catalogs, tests/golden/make_config1_pairset.py)"})
+
+    # ---- the same step with the plain all-FP64 kernel, timed the same way ----
+    plain64 = None
+    if args.variant == "filter32":
+        def step64(st_):
+            sa.rebuild_device(dA.data_ptr(), n, st_)
+            sb.rebuild_device(dB.data_ptr(), nb, st_)
+            st_.ms_match += ctx.match(sa, sb, r, xm.XM_PLAIN64, fetch=False, with_dist=args.dist)[2]["ms_match"]
+        for _ in range(max(1, args.warmup)):
+            step64(xm.XmStats())
+        st64 = xm.XmStats()
+        torch.cuda.synchronize(dev)
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(K):
+            step64(st64)
+        g1.record(stream)
+        g1.synchronize()
+        ms64 = max_over_ranks(g0.elapsed_time(g1) / K, pg, dev)
+        k64 = st64.ms_match / K
+        plain64 = {"ms_per_step": ms64, "pair_kernel_ms": k64, "value": whole_job_rate(world, n_cand, ms64),
+                   "step_speedup_vs_plain64": ms64 / ms,
+                   "kernel_speedup_vs_plain64": k64 / per["pair_kernel"] if per["pair_kernel"] > 0 else None,
+                   "what": "same step and timing, pair kernel XM_PLAIN64: FP64 cuts and both unit vectors by "
+                           "sincos for every candidate, as Worker.cu:88-97"}
 
     # ---- e2e through the C ABI with host buffers ----
     e2e_steps = args.e2e_steps or max(1, min(args.steps, 3))
@@ -411,6 +477,7 @@ def run_ours(args):
     e2e_ms = max_over_ranks(f0.elapsed_time(f1) / e2e_steps, pg, dev)
     if got != n_match:
         raise RuntimeError("e2e match count %d differs from %d" % (got, n_match))
+    pair_set["e2e_digest_equal"] = pairhash.pairset_digest(outP[:got]) == pair_set["digest"]
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -431,7 +498,8 @@ def run_ours(args):
         "border_pairs": stats.n_border // K,
         "borderline_fraction": (stats.n_border / stats.n_tested) if stats.n_tested else 0.0,
         "gpu_launches": int(stats.n_launches),
-        "roofline": roofline, "stages": stages, "pipeline_roofline": pipeline,
+        "roofline": roofline, "fp32_issue": fp32_issue, "stages": stages, "pipeline_roofline": pipeline,
+        "plain64": plain64, "pair_set": pair_set,
         "clocks": clocks,
         "e2e": {"value": whole_job_rate(world, n_cand, e2e_ms), "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 24 * (n + nb), "d2h_bytes_per_step": (24 if args.dist else 16) * n_match,
@@ -442,7 +510,7 @@ def run_ours(args):
                 "parts_ms": {k: v / e2e_steps for k, v in e2e_parts.items()}},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(A, B, r, args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(A, B, r)
     sa.free()
     sb.free()
     ctx.close()

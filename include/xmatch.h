@@ -159,7 +159,10 @@ typedef struct xm_job {
 xm_status xm_match_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags,
                          const xm_tuning *tuning, xm_pairs *outs, uint64_t *job_counts,
                          xm_stats *stats);
-/* Times a few tile/chunk settings on the batch and returns the fastest. */
+/* Times the batch under the fixed tuning {tile 128, chunk 16, zones 16}
+ * (*fixed_ms) and under 18 tile / chunk / zones settings, and returns the
+ * fastest of all of them (*best, *best_ms <= *fixed_ms).  Replaces the
+ * reference's fixed 16 x 16 launch geometry (Worker.cu:351-359). */
 xm_status xm_autotune_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t flags,
                             xm_tuning *best, float *best_ms, float *fixed_ms);
 
@@ -190,6 +193,9 @@ typedef struct xm_serve_cfg {
 typedef struct xm_serve_info {
     double t_submit_ms;    /* host clock (ms since the server opened) at submit */
     double t_admit_ms;     /* admitted (memory reserved, build started) */
+    double t_built_ms;     /* zone build finished, waiting for a batch */
+    double t_batch_ms;     /* its batch taken by the matcher (pair kernel queued) */
+    double t_matched_ms;   /* pair kernel of the batch finished, matches grouped */
     double t_done_ms;      /* results ready on the host */
     uint32_t batch;        /* batch number that matched it */
     uint32_t batch_size;   /* queries in that batch */
@@ -208,6 +214,10 @@ xm_status xm_serve_submit(xm_server *srv, const xm_obj *objs, uint64_t n, double
  * result kept) when the buffers are too small; otherwise the matches are
  * copied and the ticket is released.  A failed query returns its error once. */
 xm_status xm_serve_poll(xm_server *srv, uint64_t ticket, int wait, xm_pairs *out, xm_serve_info *info);
+/* Message of the last failed query this server returned from xm_serve_poll,
+ * copied into buf (at most cap bytes, NUL-terminated); safe to call from any
+ * thread while the server runs. */
+xm_status xm_serve_last_error(xm_server *srv, char *buf, uint64_t cap);
 /* Finishes every queued query, stops the threads and frees the server. */
 xm_status xm_serve_close(xm_server *srv);
 
@@ -231,7 +241,8 @@ xm_status xm_pairs_write(const char *path, const xm_pairs *pairs, int mode, int 
  * (XM_NOALLOC_MAX_OBJS records, about 25 MB of device memory, held by every
  * GPU that loads the library until the process exits).  Calls no cudaMalloc
  * or cudaFree and allocates nothing on the host heap.
- *   device        GPU to run on (made current for the call)
+ *   device        GPU to run on (current during the call; the caller's
+ *                 current device is restored before it returns)
  *   stream        cudaStream_t to queue on (NULL = default stream); the call
  *                 returns after the work on it has completed
  *   dev_objs      n records in device memory, n <= XM_NOALLOC_MAX_OBJS,

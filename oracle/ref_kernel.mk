@@ -3,9 +3,10 @@
 # unmodified from the read-only reference tree for sm_100a, linked with the
 # harness oracle/ref_harness.cu.  Test infrastructure only; needs the
 # reference tree, so it is built in the build container and the .so travels.
-#   make -f oracle/ref_kernel.mk
-HERE   := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
-REF    ?= /root/reference/BoostXmatch/BoostXmatch
+#   make -f oracle/ref_kernel.mk [REFERENCE=<reference checkout>]
+HERE      := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
+REFERENCE ?= /root/reference
+REF       ?= $(REFERENCE)/BoostXmatch/BoostXmatch
 OUT    := $(HERE)_ref
 NVCC   ?= nvcc
 FLAGS  := -gencode arch=compute_100a,code=sm_100a -O2 -std=c++17 -Xcompiler -fPIC \

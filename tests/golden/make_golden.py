@@ -26,7 +26,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 
-REF_DATA = "/root/reference/Data"
+# the reference checkout (XMATCH_REFERENCE overrides the build container's path)
+REF_DATA = os.path.join(os.environ.get("XMATCH_REFERENCE", "/root/reference"), "Data")
 
 
 def main():

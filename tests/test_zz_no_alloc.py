@@ -80,6 +80,63 @@ def test_noalloc_matches_regular_build(ctx):
         assert np.array_equal(xyz[:, :3], ref)
 
 
+def test_noalloc_at_capacity(ctx):
+    """Exactly XM_NOALLOC_MAX_OBJS records: the fixed scratch is full."""
+    import xmatch_b200 as xm
+    n = xm._capi.XM_NOALLOC_MAX_OBJS
+    objs = _catalog(3, n)
+    zh = 2.0 * ARCSEC
+    ids, radec, xyz, zoff = _noalloc(objs, zh)
+    seg = ctx.build(objs, zh)
+    rid, rradec, zb, ze = seg.export()
+    seg.free()
+    assert len(ids) == n - 100        # 50 NaN ra and 50 dec = 91 dropped
+    assert np.array_equal(ids, rid) and radec.tobytes() == rradec.tobytes()
+    assert np.array_equal(zoff[:-1], zb) and np.array_equal(zoff[1:], ze)
+
+
+def test_noalloc_empty_and_all_dropped(ctx):
+    """n = 0, and an input whose every record is dropped: nothing kept, every
+    zone offset 0."""
+    zh = 5.0 * ARCSEC
+    n_zones = int(np.ceil(180 / zh))
+    ids, radec, xyz, zoff = _noalloc(np.empty(0, OBJ_DTYPE), zh)
+    assert len(ids) == 0 and len(zoff) == n_zones + 1 and not zoff.any()
+    bad = _catalog(4, 5000)
+    bad["dec"] = 95.0
+    ids, radec, xyz, zoff = _noalloc(bad, zh)
+    assert len(ids) == 0 and not zoff.any()
+    # and a regular call after them still agrees with the regular build
+    objs = _catalog(5, 20_000)
+    ids, radec, xyz, zoff = _noalloc(objs, zh)
+    seg = ctx.build(objs, zh)
+    rid, rradec, zb, ze = seg.export()
+    seg.free()
+    assert np.array_equal(ids, rid) and radec.tobytes() == rradec.tobytes()
+
+
+def test_noalloc_rejects_small_zone_array_and_keeps_device(ctx):
+    import torch
+    import xmatch_b200 as xm
+    zh = 5.0 * ARCSEC
+    n_zones = int(np.ceil(180 / zh))
+    objs = _catalog(6, 1000)
+    dev = torch.device("cuda", 0)
+    d_in = torch.from_numpy(objs.view(np.uint8).copy()).to(dev)
+    out = [torch.empty(k * len(objs), dtype=t, device=dev)
+           for k, t in ((1, torch.int64), (2, torch.float64), (4, torch.float32))]
+    d_zoff = torch.empty(n_zones, dtype=torch.int32, device=dev)     # one entry short
+    torch.cuda.synchronize(dev)
+    kept = ctypes.c_uint64(12345)
+    before = torch.cuda.current_device()
+    rc = xm._lib.xm_segment_build_noalloc(0, None, ctypes.c_void_p(d_in.data_ptr()), len(objs), zh,
+                                          *[ctypes.c_void_p(t.data_ptr()) for t in out],
+                                          ctypes.c_void_p(d_zoff.data_ptr()), n_zones, ctypes.byref(kept))
+    assert rc == xm._capi.XM_ERR_INVALID
+    assert kept.value == 12345          # rejected before any work
+    assert torch.cuda.current_device() == before
+
+
 def test_noalloc_rejects_oversize(ctx):
     import xmatch_b200 as xm
     kept = ctypes.c_uint64()

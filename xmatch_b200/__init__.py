@@ -154,10 +154,16 @@ class Server:
         _check(_lib.xm_serve_open(ctx._h, catalog.handle, ctypes.byref(cfg), ctypes.byref(h)), ctx._h)
         self._h = h
 
+    def _check(self, status):
+        if status != XM_OK:
+            buf = ctypes.create_string_buffer(1024)
+            _lib.xm_serve_last_error(self._h, buf, len(buf))
+            raise XmatchError(status, buf.value.decode(errors="replace"))
+
     def submit(self, objs, sr_deg):
         objs = as_objs(objs)
         t = ctypes.c_uint64()
-        _check(_lib.xm_serve_submit(self._h, _ptr(objs), len(objs), sr_deg, ctypes.byref(t)), self.ctx._h)
+        self._check(_lib.xm_serve_submit(self._h, _ptr(objs), len(objs), sr_deg, ctypes.byref(t)))
         return t.value
 
     def poll(self, ticket, wait=True):
@@ -167,12 +173,12 @@ class Server:
         rc = _lib.xm_serve_poll(self._h, ticket, 1 if wait else 0, ctypes.byref(p), ctypes.byref(info))
         if rc == _capi.XM_ERR_BUSY:
             return None
-        _check(rc, self.ctx._h)
+        self._check(rc)
         n = p.count
         pairs = np.empty((max(n, 1), 2), np.int64)
         dist = np.empty(max(n, 1), np.float64) if self.with_dist else None
         p = XmPairs(_ptr(pairs), _ptr(dist), n, 0)
-        _check(_lib.xm_serve_poll(self._h, ticket, 1, ctypes.byref(p), ctypes.byref(info)), self.ctx._h)
+        self._check(_lib.xm_serve_poll(self._h, ticket, 1, ctypes.byref(p), ctypes.byref(info)))
         return pairs[:n], (dist[:n] if self.with_dist else None), info.as_dict()
 
     def close(self):

@@ -64,7 +64,8 @@ class XmServeCfg(ctypes.Structure):
 
 
 class XmServeInfo(ctypes.Structure):
-    _fields_ = [("t_submit_ms", ctypes.c_double), ("t_admit_ms", ctypes.c_double), ("t_done_ms", ctypes.c_double),
+    _fields_ = [("t_submit_ms", ctypes.c_double), ("t_admit_ms", ctypes.c_double), ("t_built_ms", ctypes.c_double),
+                ("t_batch_ms", ctypes.c_double), ("t_matched_ms", ctypes.c_double), ("t_done_ms", ctypes.c_double),
                 ("batch", ctypes.c_uint32), ("batch_size", ctypes.c_uint32), ("count", ctypes.c_uint64)]
 
     def as_dict(self):
@@ -118,6 +119,7 @@ SIGNATURES = {
     "xm_serve_open": (ctypes.c_int, [P, P, ctypes.POINTER(XmServeCfg), PP]),
     "xm_serve_submit": (ctypes.c_int, [P, P, U64, D, ctypes.POINTER(U64)]),
     "xm_serve_poll": (ctypes.c_int, [P, U64, ctypes.c_int, ctypes.POINTER(XmPairs), ctypes.POINTER(XmServeInfo)]),
+    "xm_serve_last_error": (ctypes.c_int, [P, ctypes.c_char_p, U64]),
     "xm_serve_close": (ctypes.c_int, [P]),
 }
 

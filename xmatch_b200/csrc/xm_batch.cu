@@ -206,17 +206,18 @@ extern "C" xm_status xm_autotune_batch(xm_ctx *ctx, const xm_job *jobs, uint32_t
     const uint32_t tiles[] = {64, 128, 256};
     const uint32_t chunks[] = {4, 16};
     const uint32_t zones[] = {4, 16, 64};
-    float bms = 1e30f;
+    // fixed-tile reference point: tile 128, 16 zones per item, 16 tiles per claim;
+    // it is the starting best, so the setting returned is never slower than it
+    // as measured here
     xm_tuning b = {128, 16, 0, 16};
     float fixed = 0;
-    // fixed-tile reference point: tile 128, 16 zones per item, 16 tiles per claim
     {
-        xm_tuning t = {128, 16, 0, 16};
         float ms = 0;
-        XM_TRY(xm_run_jobs(ctx, jobs, n_jobs, flags, &t, n_jobs > 1, nullptr, &ms));   // warm (and size the output)
-        XM_TRY(xm_run_jobs(ctx, jobs, n_jobs, flags, &t, n_jobs > 1, nullptr, &ms));
+        XM_TRY(xm_run_jobs(ctx, jobs, n_jobs, flags, &b, n_jobs > 1, nullptr, &ms));   // warm (and size the output)
+        XM_TRY(xm_run_jobs(ctx, jobs, n_jobs, flags, &b, n_jobs > 1, nullptr, &ms));
         fixed = ms;
     }
+    float bms = fixed;
     for (uint32_t tl : tiles)
         for (uint32_t ch : chunks)
             for (uint32_t zn : zones) {

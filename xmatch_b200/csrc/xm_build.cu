@@ -1013,6 +1013,25 @@ constexpr int kNaMaxDevices = 64;
 void *g_noalloc_ptr[kNaMaxDevices] = {};
 std::mutex g_noalloc_mu;
 
+// Makes `device` current for the call and gives the caller's current device
+// back on every return path.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int device)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            cudaGetLastError();
+            prev = -1;
+        }
+        ok = cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace
 
 extern "C" xm_status xm_segment_build_noalloc(int device, void *stream, const xm_obj *objs, uint64_t n,
@@ -1031,7 +1050,8 @@ extern "C" xm_status xm_segment_build_noalloc(int device, void *stream, const xm
     int raq_bits, passes;
     xm_raq_layout(nz, &raq_bits, &passes);
     if (passes > kMaxPasses) return XM_ERR_INVALID;
-    if (cudaSetDevice(device) != cudaSuccess) return XM_ERR_CUDA;
+    DeviceGuard dg(device);
+    if (!dg.ok) return XM_ERR_CUDA;
     // one-time set-up per device: device address of the scratch array
     void *base = nullptr;
     {

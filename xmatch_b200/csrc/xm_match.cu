@@ -1059,7 +1059,10 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
         int s = 0;
         uint32_t phase = 0;
         bool ok = true;
-        int issued = 0;
+        // stages whose latest copy may still be landing (bit per stage), and the
+        // fill parity each was issued with: a stage's bit is cleared once its
+        // consumers have released it, which they do only after its copy landed
+        uint32_t pend = 0, pend_par = 0;
         int cached_job = -1;
         const double2 *a_radec = nullptr, *b_radec = nullptr;
         const float4 *a_xyz = nullptr, *b_xyz = nullptr;
@@ -1070,6 +1073,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
         // issue plan words w[16] into the next stage
         auto issue = [&](const uint32_t (&w)[16]) -> bool {
             if (!mbar_wait(&empty[s], phase ^ 1u)) return false;
+            pend &= ~(1u << s);
             if (lane == 0) {
                 const uint32_t a_start = w[0], a_len = w[1], mode = w[2] & 255u, nseg = (w[2] >> 8) & 255u;
                 const int zf = (int)w[3];
@@ -1153,7 +1157,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 }
             }
             __syncwarp();
-            issued++;
+            pend |= 1u << s;
+            pend_par = (pend_par & ~(1u << s)) | (phase << s);
             if (++s == kStages) {
                 s = 0;
                 phase ^= 1u;
@@ -1210,14 +1215,10 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             __syncwarp();
         } else {
             if (lane == 0) atomicExch(&out.counters[7], 1ull);
-            // wait (bounded) for copies still landing in the stages before leaving
-            for (int q = 0; q < kStages && q < issued; ++q) {
-                if (++s == kStages) {
-                    s = 0;
-                    phase ^= 1u;
-                }
-                mbar_wait(&full[s], phase);
-            }
+            // wait (bounded) for the copies that may still be landing in the
+            // stages, each on the parity it was issued with, before leaving
+            for (int q = 0; q < kStages; ++q)
+                if (pend & (1u << q)) mbar_wait(&full[q], (pend_par >> q) & 1u);
         }
         return;
     }

@@ -17,6 +17,7 @@
 // the builder's stream while that batch runs, and joins the next batch.  The
 // pair set of a query does not depend on its batch: each job is matched by the
 // same kernel over the same two segments as xm_match.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -66,6 +67,7 @@ struct xm_server {
     uint64_t next_ticket = 1;
     uint64_t in_flight = 0;        // reserved bytes of admitted queries
     uint32_t n_batches = 0;
+    std::string last_error;        // message of the last failed query polled (guarded by mu)
     bool stop = false, builder_done = false;
     std::thread builder, matcher;
     std::vector<int64_t> hp;       // host staging of a batch's pairs
@@ -130,6 +132,7 @@ void builder_loop(xm_server *S)
         } else {
             q->seg = seg;
             q->state = Q_BUILT;
+            q->info.t_built_ms = S->now_ms();
             S->ready.push_back(q);
         }
         S->cv.notify_all();
@@ -144,9 +147,11 @@ void matcher_loop(xm_server *S)
             std::unique_lock<std::mutex> lk(S->mu);
             S->cv.wait(lk, [&] { return !S->ready.empty() || S->builder_done; });
             if (S->ready.empty() && S->builder_done) return;
+            const double t = S->now_ms();
             while (!S->ready.empty() && batch.size() < S->cfg.max_batch) {
                 batch.push_back(S->ready.front());
                 S->ready.pop_front();
+                batch.back()->info.t_batch_ms = t;
             }
         }
         const uint32_t nb = (uint32_t)batch.size();
@@ -164,6 +169,7 @@ void matcher_loop(xm_server *S)
                 ctx->res.grouped = false;
             }
         }
+        const double t_matched = S->now_ms();
         uint64_t total = 0;
         if (rc == XM_OK) {
             total = ctx->res.count;
@@ -199,6 +205,7 @@ void matcher_loop(xm_server *S)
             }
             q.info.batch = b;
             q.info.batch_size = nb;
+            q.info.t_matched_ms = t_matched;
             q.info.t_done_ms = t;
             S->in_flight -= q.bytes;
             S->garbage.push_back(q.seg);
@@ -279,7 +286,7 @@ extern "C" xm_status xm_serve_poll(xm_server *S, uint64_t ticket, int wait, xm_p
     }
     if (info) *info = q->info;
     if (q->state == Q_FAILED) {
-        S->mctx->last_error = q->msg;
+        S->last_error = q->msg;   // the matcher thread owns mctx; the text is kept per server
         S->tickets.erase(it);
         return q->err;
     }
@@ -294,6 +301,16 @@ extern "C" xm_status xm_serve_poll(xm_server *S, uint64_t ticket, int wait, xm_p
     if (out->pairs && c) std::memcpy(out->pairs, q->pairs.data(), c * 16);
     if (out->dist && c) std::memcpy(out->dist, q->dist.data(), c * 8);
     S->tickets.erase(it);
+    return XM_OK;
+}
+
+extern "C" xm_status xm_serve_last_error(xm_server *S, char *buf, uint64_t cap)
+{
+    if (!S || !buf || cap == 0) return XM_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(S->mu);
+    const size_t n = std::min<size_t>(S->last_error.size(), (size_t)cap - 1);
+    std::memcpy(buf, S->last_error.data(), n);
+    buf[n] = 0;
     return XM_OK;
 }
 

@@ -6,7 +6,9 @@ distribution and seed.
 """
 import numpy as np
 
-from . import OBJ_DTYPE
+# .idradec record (Obj.h:21-25), 24 bytes; defined here too so that this file
+# also loads on its own (by path), without the package and its library
+OBJ_DTYPE = np.dtype([("id", "<i8"), ("ra", "<f8"), ("dec", "<f8")])
 
 ARCSEC = 1.0 / 3600.0
 
