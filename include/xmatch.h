@@ -130,6 +130,27 @@ xm_status xm_segment_free(xm_segment *seg);
 /* Segment fields (Segment.h:24-26): kept objects, zone count, zone height. */
 xm_status xm_segment_info(const xm_segment *seg, uint32_t *seg_id, uint64_t *n_kept,
                           int32_t *n_zones, double *zh_deg);
+/* ---- segments held in host memory (catalogs larger than device memory) ----
+ * The reference keeps every segment in host RAM and copies the two of a job to
+ * the GPU when the job runs (Worker.cu:251-292, BoostXmatch.cpp:247-274).
+ * Here a built segment can be moved to pinned host memory and paged back in
+ * per job; xm_match / xm_match_batch refuse an offloaded segment
+ * (XM_ERR_INVALID).
+ *   xm_segment_offload   copy the sorted arrays to pinned host memory (kept by
+ *                        the segment) and free the device copy
+ *   xm_segment_page_in   queue the copy back to device memory on the
+ *                        context's second stream and return at once; work
+ *                        queued on a context after that waits for the copy, so
+ *                        paging the next job's segment in overlaps the current
+ *                        match
+ *   xm_segment_page_out  free the device copy (after the work already queued on
+ *                        it), keeping the host copy
+ *   xm_segment_resident  whether the arrays are in device memory, and their size
+ * Rebuilding a segment drops its host copy. */
+xm_status xm_segment_offload(xm_segment *seg);
+xm_status xm_segment_page_in(xm_segment *seg);
+xm_status xm_segment_page_out(xm_segment *seg);
+xm_status xm_segment_resident(const xm_segment *seg, int *on_device, uint64_t *bytes);
 /* Copy the sorted segment to the host, as Sorter.cu:178-182 fills
  * Segment::vId, vRadec, vZoneBegin, vZoneEnd.  Any pointer may be NULL.
  * radec: [2*n_kept] radians; zone_begin/zone_end: [n_zones]. */

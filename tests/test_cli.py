@@ -1,6 +1,7 @@
 """The command-line driver (xmatch_b200/bin/xmatch, options and flow of
 BoostXmatch.x): argument handling on the CPU, pair files against the oracle on
-the GPU, whole and in segments (resident A segments x rounds of B segments)."""
+the GPU, whole and in segments (A segments resident in device memory, or held
+in host memory and paged in per job, x rounds of B segments)."""
 import os
 import subprocess
 
@@ -68,3 +69,25 @@ def test_pairs_equal_the_oracle(tmp_path, numobj):
     assert np.max(np.abs(q["d"] - do), initial=0) <= 1e-12
     if numobj:
         assert len(os.listdir(out)) == (len(B) + 299) // 300       # one file per worker per round
+
+
+@pytest.mark.gpu
+def test_fileA_larger_than_the_device_budget(tmp_path):
+    """fileA's segments exceed --resident-mb: they are held in pinned host memory
+    and paged in one job at a time (the reference's host-resident segments,
+    BoostXmatch.cpp:247-274); the pair files equal the oracle's."""
+    fa, fb = os.path.join(GOLD, "test.idradec"), os.path.join(GOLD, "test2.idradec")
+    A, B = np.fromfile(fa, oracle.OBJ_DTYPE), np.fromfile(fb, oracle.OBJ_DTYPE)
+    for r_arcsec in (5, 30):
+        po, do, _ = oracle.xmatch(A, B, r_arcsec * ARCSEC)
+        po = po[np.lexsort((po[:, 1], po[:, 0]))]
+        out = tmp_path / ("paged%d" % r_arcsec)
+        # 10,000 A records in 34 segments of 300 (each with its zone offsets, about 0.5 MB at zh = 5")
+        # against a 0.1 MiB budget; B (1,000 records) in 4 rounds of 300, which alternate the order of
+        # the A segments
+        r = run("-r", str(r_arcsec), "-n", "300", "--resident-mb", "0.1", "-v", "1", "-o", str(out), fa, fb)
+        assert r.returncode == 0, r.stderr
+        assert "paged in per job" in r.stderr
+        p = np.concatenate(read_pairs(out, 16))
+        p = p[np.lexsort((p[:, 1], p[:, 0]))]
+        assert np.array_equal(p, po)

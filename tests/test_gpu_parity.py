@@ -357,3 +357,33 @@ def test_segmentation_invariance(ctx, fixtures):
     assert np.array_equal(sp(allp), sp(whole))
     for s in segs:
         s.free()
+
+
+def test_offloaded_segments_page_in_per_job(ctx, fixtures):
+    """Segments moved to pinned host memory and paged back in (the next one's copy
+    queued while the current job matches) give the pairs of resident segments;
+    an offloaded segment is refused by the match and still exports."""
+    import xmatch_b200 as xm
+    a, a2 = fixtures
+    zh = 5 * ARCSEC
+    segs = [ctx.build(a[s:s + 2500], zh, k) for k, s in enumerate(range(0, len(a), 2500))]
+    B = ctx.build(a2, zh, 9)
+    want = [sp(ctx.match(s, B, zh, xm.XM_NO_DIST)[0]) for s in segs]
+    ids0 = segs[0].export()
+    for s in segs:
+        s.offload()
+        assert s.resident()[0] is False
+    assert np.array_equal(segs[0].export()[0], ids0[0])     # from the host copy
+    with pytest.raises(xm.XmatchError):
+        ctx.match(segs[0], B, zh)
+    for rep in range(2):
+        segs[0].page_in()
+        for k, s in enumerate(segs):
+            if k + 1 < len(segs):
+                segs[k + 1].page_in()
+            p = sp(ctx.match(s, B, zh, xm.XM_NO_DIST)[0])
+            assert np.array_equal(p, want[k]), (rep, k)
+            s.page_out()
+    for s in segs:
+        s.free()
+    B.free()

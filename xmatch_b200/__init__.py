@@ -127,6 +127,25 @@ class DeviceSegment:
         _check(_lib.xm_segment_rebuild_device(self.handle, ctypes.c_void_p(dev_ptr), n,
                                               ctypes.byref(stats) if stats is not None else None), self._ctx._h)
 
+    # ---- host-resident segments (catalogs larger than device memory) ----
+    def offload(self):
+        """Move the sorted arrays to pinned host memory and free the device copy."""
+        _check(_lib.xm_segment_offload(self.handle), self._ctx._h)
+
+    def page_in(self):
+        """Queue the copy back to the device (returns at once; later work waits for it)."""
+        _check(_lib.xm_segment_page_in(self.handle), self._ctx._h)
+
+    def page_out(self):
+        """Free the device copy, keeping the host copy."""
+        _check(_lib.xm_segment_page_out(self.handle), self._ctx._h)
+
+    def resident(self):
+        """(arrays in device memory, their bytes)."""
+        on, nb = ctypes.c_int(), ctypes.c_uint64()
+        _check(_lib.xm_segment_resident(self.handle, ctypes.byref(on), ctypes.byref(nb)))
+        return bool(on.value), nb.value
+
     def free(self):
         if self._h is not None:
             _lib.xm_segment_free(self._h)

@@ -97,6 +97,10 @@ SIGNATURES = {
     "xm_segment_build_device": (ctypes.c_int, [P, U32, P, U64, D, PP, ctypes.POINTER(XmStats)]),
     "xm_segment_rebuild_device": (ctypes.c_int, [P, P, U64, ctypes.POINTER(XmStats)]),
     "xm_segment_free": (ctypes.c_int, [P]),
+    "xm_segment_offload": (ctypes.c_int, [P]),
+    "xm_segment_page_in": (ctypes.c_int, [P]),
+    "xm_segment_page_out": (ctypes.c_int, [P]),
+    "xm_segment_resident": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(U64)]),
     "xm_segment_info": (ctypes.c_int, [P, ctypes.POINTER(U32), ctypes.POINTER(U64), ctypes.POINTER(I32),
                                        ctypes.POINTER(D)]),
     "xm_segment_export": (ctypes.c_int, [P, P, P, P, P]),

@@ -135,6 +135,21 @@ xm_status xm_dev_alloc(xm_ctx *ctx, void **p, size_t bytes)
     return XM_OK;
 }
 
+xm_status xm_dev_alloc_on(xm_ctx *ctx, void **p, size_t bytes, cudaStream_t st)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->last_error = std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
+                          cudaGetErrorString(e);
+        *p = nullptr;
+        return XM_ERR_NOMEM;
+    }
+    return XM_OK;
+}
+
 void xm_dev_free(xm_ctx *ctx, void *p)
 {
     if (p) cudaFreeAsync(p, ctx->stream);
@@ -459,8 +474,84 @@ extern "C" xm_status xm_segment_free(xm_segment *seg)
     if (!seg) return XM_OK;
     xm_ctx *ctx = seg->ctx;
     cudaSetDevice(ctx->device);
+    if (seg->ready_pending) cudaStreamWaitEvent(ctx->stream, seg->ready, 0);
     xm_dev_free(ctx, seg->store);
+    if (seg->host_store || seg->ready) {
+        cudaStreamSynchronize(ctx->stream2);   // a page-in copy may still read the host copy
+        if (seg->host_store) cudaFreeHost(seg->host_store);
+        if (seg->ready) cudaEventDestroy(seg->ready);
+    }
     delete seg;
+    return XM_OK;
+}
+
+// ---- segments in host memory (replaces the reference's per-job copies of
+// host-resident segments to the GPU, Worker.cu:251-292, for catalogs larger
+// than device memory) ----
+
+extern "C" xm_status xm_segment_offload(xm_segment *seg)
+{
+    if (!seg) return XM_ERR_INVALID;
+    xm_ctx *ctx = seg->ctx;
+    cudaSetDevice(ctx->device);
+    if (!seg->store) return XM_OK;   // already offloaded
+    if (seg->ready_pending) XM_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, seg->ready, 0));
+    seg->ready_pending = false;
+    if (!seg->host_store) {
+        if (cudaMallocHost(&seg->host_store, seg->store_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            seg->host_store = nullptr;
+            ctx->last_error = "pinned host allocation of " + std::to_string(seg->store_bytes) + " bytes failed";
+            return XM_ERR_NOMEM;
+        }
+        XM_CUDA(ctx, cudaMemcpyAsync(seg->host_store, seg->store, seg->store_bytes, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+        XM_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    xm_dev_free(ctx, seg->store);   // after the work queued on the segment
+    seg->store = nullptr;
+    xm_seg_layout(seg, nullptr);
+    return XM_OK;
+}
+
+extern "C" xm_status xm_segment_page_in(xm_segment *seg)
+{
+    if (!seg) return XM_ERR_INVALID;
+    xm_ctx *ctx = seg->ctx;
+    cudaSetDevice(ctx->device);
+    if (seg->store) return XM_OK;
+    if (!seg->host_store) return XM_ERR_INVALID;
+    if (!seg->ready) XM_CUDA(ctx, cudaEventCreateWithFlags(&seg->ready, cudaEventDisableTiming));
+    void *p = nullptr;
+    XM_TRY(xm_dev_alloc_on(ctx, &p, seg->store_bytes, ctx->stream2));
+    XM_CUDA(ctx, cudaMemcpyAsync(p, seg->host_store, seg->store_bytes, cudaMemcpyHostToDevice, ctx->stream2));
+    XM_CUDA(ctx, cudaEventRecord(seg->ready, ctx->stream2));
+    seg->ready_pending = true;
+    seg->store = p;
+    xm_seg_layout(seg, p);
+    return XM_OK;
+}
+
+extern "C" xm_status xm_segment_page_out(xm_segment *seg)
+{
+    if (!seg) return XM_ERR_INVALID;
+    if (!seg->store) return XM_OK;
+    if (!seg->host_store) return xm_segment_offload(seg);
+    xm_ctx *ctx = seg->ctx;
+    cudaSetDevice(ctx->device);
+    if (seg->ready_pending) XM_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, seg->ready, 0));
+    seg->ready_pending = false;
+    xm_dev_free(ctx, seg->store);   // stream-ordered after the work queued on the segment
+    seg->store = nullptr;
+    xm_seg_layout(seg, nullptr);
+    return XM_OK;
+}
+
+extern "C" xm_status xm_segment_resident(const xm_segment *seg, int *on_device, uint64_t *bytes)
+{
+    if (!seg) return XM_ERR_INVALID;
+    if (on_device) *on_device = seg->store != nullptr;
+    if (bytes) *bytes = seg->store_bytes;
     return XM_OK;
 }
 
@@ -482,11 +573,16 @@ extern "C" xm_status xm_segment_export(const xm_segment *seg, int64_t *id, doubl
     xm_ctx *ctx = seg->ctx;
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
-    if (id && seg->n) XM_CUDA(ctx, cudaMemcpyAsync(id, seg->id, seg->n * 8, cudaMemcpyDeviceToHost, st));
-    if (radec && seg->n) XM_CUDA(ctx, cudaMemcpyAsync(radec, seg->radec, seg->n * 16, cudaMemcpyDeviceToHost, st));
+    if (!seg->store && !seg->host_store) return XM_ERR_INVALID;
+    if (seg->ready_pending) XM_CUDA(ctx, cudaStreamWaitEvent(st, seg->ready, 0));
+    // the device arrays, or the host copy of an offloaded segment
+    const char *base = seg->store ? (const char *)seg->store : (const char *)seg->host_store;
+    const void *s_id = base + seg->off_id, *s_radec = base + seg->off_radec, *s_zoff = base;
+    if (id && seg->n) XM_CUDA(ctx, cudaMemcpyAsync(id, s_id, seg->n * 8, cudaMemcpyDefault, st));
+    if (radec && seg->n) XM_CUDA(ctx, cudaMemcpyAsync(radec, s_radec, seg->n * 16, cudaMemcpyDefault, st));
     if (zone_begin || zone_end) {
         std::vector<uint32_t> z((size_t)seg->n_zones + 1);
-        XM_CUDA(ctx, cudaMemcpyAsync(z.data(), seg->zone_off, z.size() * 4, cudaMemcpyDeviceToHost, st));
+        XM_CUDA(ctx, cudaMemcpyAsync(z.data(), s_zoff, z.size() * 4, cudaMemcpyDefault, st));
         XM_CUDA(ctx, cudaStreamSynchronize(st));
         for (int32_t k = 0; k < seg->n_zones; ++k) {
             if (zone_begin) zone_begin[k] = (int32_t)z[k];
@@ -540,6 +636,12 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
             ctx->last_error = "job " + std::to_string(j) + ": zone heights differ";
             return XM_ERR_MISMATCH;
         }
+        if (!A->store || !B->store) {
+            ctx->last_error = "job " + std::to_string(j) + ": a segment is offloaded (xm_segment_page_in it first)";
+            return XM_ERR_INVALID;
+        }
+        for (const xm_segment *s : {A, B})   // a page-in copy of the segment must land first
+            if (s->ready_pending) XM_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, s->ready, 0));
         xm_match_params p;
         if (xm_make_params(jobs[j].sr_deg, A->zh_deg, &p) != XM_OK) {
             ctx->last_error = "job " + std::to_string(j) + ": invalid radius";
@@ -550,12 +652,10 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
         d.a_id = (const long long *)A->id;
         d.a_radec = A->radec;
         d.a_xyz = A->xyz;
-        d.a_xyz64 = A->xyz64;
         d.a_zoff = A->zone_off;
         d.b_id = (const long long *)B->id;
         d.b_radec = B->radec;
         d.b_xyz = B->xyz;
-        d.b_xyz64 = B->xyz64;
         d.b_zoff = B->zone_off;
         d.sr_rad = p.sr_rad;
         d.sr_dist2 = p.sr_dist2;

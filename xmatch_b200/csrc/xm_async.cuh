@@ -1,0 +1,79 @@
+// xm_async.cuh -- shared-memory mbarriers and bulk asynchronous copies
+// (cp.async.bulk, global -> shared of the issuing CTA, no multicast), used by
+// the zone builder's record streaming and the pair kernel's staging ring.
+// Every wait is bounded: a wait that runs out returns false and the caller
+// reports an error instead of spinning for ever.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace xm {
+
+constexpr unsigned kWaitLimit = 1u << 26;   // polls of a bounded mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this thread's earlier generic-proxy accesses of shared memory before
+// later async-proxy (bulk copy) writes to it.
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// bytes (a multiple of 16) from global src (16-byte aligned) to shared dst
+// (16-byte aligned), completion counted on bar.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for the phase of the given parity; false if it did not complete
+// within the limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
+{
+    for (unsigned it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
+}  // namespace xm

@@ -10,8 +10,8 @@
 //                          the zone begin/end of Sorter.cu:156-165
 //   id[n]                  int64
 //   radec[n]               double2 radians, deg / RAD2DEG (Sorter.cu:52-62)
-//   xyz[n]                 float4: FP32 unit vector, w = raq bits
-//   xyz64[3n]              FP64 unit vector (the project sincos, Worker.cu:31-40)
+//   xyz[n]                 float4: FP32 unit vector (the project sincos,
+//                          Worker.cu:31-40, rounded to FP32), w = raq bits
 // zone = floor((dec + 90) / zh) (Sorter.cu:20-24); raq = the leading 27
 // bits of floor(ra_rad * 2^31 / pi), a monotone quantisation of ra (its
 // step is 2 pi / 2^27, 4.7e-8 rad), so within a zone
@@ -34,6 +34,7 @@
 #include <mutex>
 #include <vector>
 
+#include "xm_async.cuh"
 #include "xm_internal.h"
 #include "xm_math.cuh"
 
@@ -245,8 +246,7 @@ rs_downsweep(const unsigned long long *__restrict__ keys_in, const uint32_t *__r
 
 __global__ void zb_gather(const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ vals,
                           const xm_obj *__restrict__ objs, unsigned long long n_kept, unsigned long long raq_mask,
-                          long long *__restrict__ id, double2 *__restrict__ radec, float4 *__restrict__ xyz,
-                          double *__restrict__ xyz64)
+                          long long *__restrict__ id, double2 *__restrict__ radec, float4 *__restrict__ xyz)
 {
     for (unsigned long long j = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; j < n_kept;
          j += (unsigned long long)gridDim.x * blockDim.x) {
@@ -259,11 +259,6 @@ __global__ void zb_gather(const unsigned long long *__restrict__ keys, const uin
         radec[j] = make_double2(ra, dec);
         xyz[j] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z),
                              __uint_as_float((uint32_t)(keys[j] & raq_mask)));
-        if (xyz64) {
-            xyz64[3 * j] = x;
-            xyz64[3 * j + 1] = y;
-            xyz64[3 * j + 2] = z;
-        }
     }
 }
 
@@ -298,16 +293,18 @@ __global__ void zb_bounds_fill(const unsigned long long *__restrict__ keys, unsi
 
 // ---------------------------------------------------------------------------
 // Zone-bucket build.
-//   zc_count     objects per zone (and the populated range, dropped count)
-//   scan         zone offsets
-//   zc_classify  bucket cursors, list of zones above kWarpZone objects
-//   zc_scatter   32-byte records into buckets of 2^bucket_shift consecutive
-//                zones (per-bucket atomic cursors; few enough buckets that
-//                their write fronts stay in L2)
-//   zs_bucket    one block per bucket: records into zone order (shared-memory
-//                cursors, writes stay inside the bucket), then each zone of at
-//                most kWarpZone objects sorted by (raq, input index) by one
-//                warp and written out as the segment's SoA
+//   zc_count     objects per bucket of 2^bucket_shift consecutive zones (a
+//                shared-memory histogram per block), the populated zone range
+//                and the dropped count; reads ra and dec only
+//   scan         bucket offsets (the buckets' atomic cursors)
+//   zc_scatter   records streamed through shared memory (bulk async copies),
+//                each kept record into its bucket as a 32-byte ZRec through
+//                the bucket cursors (few enough buckets that their write
+//                fronts stay in L2)
+//   zs_bucket    one block per bucket: zone counts and offsets, the bucket's
+//                (raq, input index) keys into zone order in shared memory,
+//                each zone of at most kWarpZone objects ranked by one warp and
+//                written out as the segment's SoA
 //   zs_block     zones of kWarpZone+1 .. kBlockZone objects: bitonic sort of a
 //                block
 // Zones above kBlockZone objects send the segment to the radix-sort build.
@@ -325,6 +322,100 @@ struct ZRec {          // 32 bytes, one per kept object
     uint32_t idx;      // input index
 };
 constexpr uint32_t kRaqMask = (1u << kRaqBits) - 1u;
+
+// ---- record tiles streamed through shared memory (scatter pass) ----
+// A block walks its tiles of kTileRecs records through two shared-memory
+// buffers.  A full tile of a 16-byte aligned input is one bulk asynchronous
+// copy (cp.async.bulk, completion counted on the buffer's mbarrier), issued
+// while the previous tile is processed; a partial last tile, or a tile of an
+// input that is only 8-byte aligned, is copied by the block's threads.
+constexpr int kStageThreads = 256;
+constexpr int kPerThread = 8;                              // records per thread per tile
+constexpr int kTileRecs = kStageThreads * kPerThread;      // 2048 records, 48 KB
+constexpr uint32_t kTileBytes = kTileRecs * 24u;
+
+struct TileRing {
+    unsigned long long w[2][kTileRecs * 3];   // raw records: id, ra bits, dec bits
+    uint64_t bar[2];
+};
+
+__device__ __forceinline__ double rec_ra(const unsigned long long *w, uint32_t i)
+{
+    return __longlong_as_double((long long)w[3 * i + 1]);
+}
+__device__ __forceinline__ double rec_dec(const unsigned long long *w, uint32_t i)
+{
+    return __longlong_as_double((long long)w[3 * i + 2]);
+}
+
+// Zone of a record; -1 if it is dropped (zone outside the sphere, non-finite ra).
+__device__ __forceinline__ int rec_zone(double ra_deg, double dec_deg, const KeyParams &kp)
+{
+    return isfinite(ra_deg) ? xm::zone_of(dec_deg, kp.zh_deg, kp.n_zones) : -1;
+}
+
+// Calls f(first record, count, records in shared memory) for every tile of the
+// block (tiles blockIdx.x, blockIdx.x + gridDim.x, ...).  Returns false (the
+// same on every thread) if a bounded wait for a bulk copy ran out; the copies
+// still in flight have then been waited for (bounded) before returning.
+template <class F>
+__device__ bool for_each_tile(const xm_obj *__restrict__ objs, unsigned long long n, bool bulk_ok, TileRing &R,
+                              F f)
+{
+    const unsigned long long n_tiles = (n + kTileRecs - 1) / kTileRecs;
+    const unsigned long long step = gridDim.x;
+    auto bulk = [&](unsigned long long t) { return bulk_ok && (t + 1) * kTileRecs <= n; };
+    if (threadIdx.x == 0) {
+        xm::mbar_init(&R.bar[0], 1);
+        xm::mbar_init(&R.bar[1], 1);
+        xm::fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t par = 0;        // bit b: parity of buffer b's next phase
+    uint32_t pend = 0;       // bit b: a bulk copy into buffer b is in flight
+    auto issue = [&](unsigned long long t, int b) {   // thread 0
+        xm::fence_proxy_async();
+        xm::mbar_expect_tx(&R.bar[b], kTileBytes);
+        xm::bulk_g2s(R.w[b], objs + t * kTileRecs, kTileBytes, &R.bar[b]);
+    };
+    unsigned long long t = blockIdx.x;
+    if (t < n_tiles && bulk(t)) {
+        if (threadIdx.x == 0) issue(t, 0);
+        pend |= 1u;
+    }
+    bool ok = true;
+    for (int b = 0; t < n_tiles; t += step, b ^= 1) {
+        const unsigned long long tn = t + step;
+        if (tn < n_tiles && bulk(tn)) {   // the other buffer was released by the last __syncthreads
+            if (threadIdx.x == 0) issue(tn, b ^ 1);
+            pend |= 2u >> b;
+        }
+        const uint32_t cnt = (uint32_t)min((unsigned long long)kTileRecs, n - t * kTileRecs);
+        if (bulk(t)) {
+            const bool got = xm::mbar_wait(&R.bar[b], (par >> b) & 1u);
+            par ^= 1u << b;
+            pend &= ~(1u << b);
+            if (!__syncthreads_and(got)) {
+                ok = false;
+                pend |= 1u << b;
+                par ^= 1u << b;
+                break;
+            }
+        } else {
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(objs + t * kTileRecs);
+            for (uint32_t i = threadIdx.x; i < 3 * cnt; i += blockDim.x) R.w[b][i] = __ldg(src + i);
+            __syncthreads();
+        }
+        f(t * kTileRecs, cnt, R.w[b]);
+        __syncthreads();
+    }
+    if (!ok) {   // drain: wait (bounded) for the copies still in flight
+        for (int b = 0; b < 2; ++b)
+            if (pend & (1u << b)) xm::mbar_wait(&R.bar[b], (par >> b) & 1u);
+        __syncthreads();
+    }
+    return ok;
+}
 
 // Lanes whose value equals the previous lane's form runs (consecutive equal
 // zones, as in dec-ordered input); the run's first lane acts for the run.
@@ -348,13 +439,22 @@ __device__ __forceinline__ Run warp_run(int v, unsigned lane)
     return r;
 }
 
-constexpr int kScatterU = 4;   // records per lane per iteration (independent atomics in flight)
+// Pass 1: objects per bucket of 2^shift zones (a shared-memory histogram when
+// the buckets fit, else run-aggregated global atomics), the populated zone
+// range (misc[0], misc[1]) and the dropped count (misc[2]).  Only ra and dec
+// of each record are read.
+constexpr int kCountU = 8;                // records per lane per iteration
+constexpr int kHistMax = 24 * 1024;       // buckets of a shared-memory histogram (96 KB)
 
-// Pass 1: objects per zone; populated zone range and dropped count in misc.
-__global__ void zc_count(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp,
-                         uint32_t *__restrict__ cnt, uint32_t *__restrict__ misc)
+template <bool SMEM>
+__global__ void __launch_bounds__(256)
+zc_count(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp, int shift, int n_buckets,
+         uint32_t *__restrict__ bcnt, uint32_t *__restrict__ misc)
 {
+    extern __shared__ uint32_t s_hist[];   // [n_buckets] when SMEM
     __shared__ unsigned s_lo, s_hi, s_bad;
+    if (SMEM)
+        for (int i = threadIdx.x; i < n_buckets; i += blockDim.x) s_hist[i] = 0;
     if (threadIdx.x == 0) {
         s_lo = 0xFFFFFFFFu;
         s_hi = 0u;
@@ -363,30 +463,42 @@ __global__ void zc_count(const xm_obj *__restrict__ objs, unsigned long long n, 
     __syncthreads();
     const unsigned lane = threadIdx.x & 31;
     unsigned zlo = 0xFFFFFFFFu, zhi = 0u, bad = 0u;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x * kScatterU;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x * kCountU;
     const unsigned long long warp0 =
-        (((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull) * kScatterU;
+        (((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull) * kCountU;
     for (unsigned long long wb = warp0; wb < n; wb += stride) {
-        int z[kScatterU];
+        double ra[kCountU], dec[kCountU];
 #pragma unroll
-        for (int u = 0; u < kScatterU; ++u) {
+        for (int u = 0; u < kCountU; ++u) {
             const unsigned long long i = wb + 32u * u + lane;
-            z[u] = -2;
+            ra[u] = 0.0;
+            dec[u] = 0.0;
             if (i < n) {
-                const xm_obj o = objs[i];
-                z[u] = isfinite(o.ra_deg) ? xm::zone_of(o.dec_deg, kp.zh_deg, kp.n_zones) : -1;
+                ra[u] = __ldg(&objs[i].ra_deg);
+                dec[u] = __ldg(&objs[i].dec_deg);
             }
         }
 #pragma unroll
-        for (int u = 0; u < kScatterU; ++u) {
-            if (z[u] == -1) {
-                ++bad;
-            } else if (z[u] >= 0) {
-                zlo = min(zlo, (unsigned)z[u]);
-                zhi = max(zhi, (unsigned)z[u]);
+        for (int u = 0; u < kCountU; ++u) {
+            const unsigned long long i = wb + 32u * u + lane;
+            int bk = -2;
+            if (i < n) {
+                const int z = rec_zone(ra[u], dec[u], kp);
+                if (z < 0) {
+                    ++bad;
+                    bk = -1;
+                } else {
+                    zlo = min(zlo, (unsigned)z);
+                    zhi = max(zhi, (unsigned)z);
+                    bk = z >> shift;
+                }
             }
-            const Run r = warp_run(z[u], lane);
-            if (r.is_head && z[u] >= 0) atomicAdd(&cnt[z[u]], r.len);
+            if (SMEM) {
+                if (bk >= 0) atomicAdd(&s_hist[bk], 1u);
+            } else {
+                const Run r = warp_run(bk, lane);
+                if (r.is_head && bk >= 0) atomicAdd(&bcnt[bk], r.len);
+            }
         }
     }
     zlo = __reduce_min_sync(0xffffffffu, zlo);
@@ -398,6 +510,11 @@ __global__ void zc_count(const xm_obj *__restrict__ objs, unsigned long long n, 
         atomicAdd(&s_bad, bad);
     }
     __syncthreads();
+    if (SMEM)
+        for (int i = threadIdx.x; i < n_buckets; i += blockDim.x) {
+            const uint32_t v = s_hist[i];
+            if (v) atomicAdd(&bcnt[i], v);
+        }
     if (threadIdx.x == 0) {
         if (s_lo != 0xFFFFFFFFu) atomicMin(&misc[0], s_lo);
         atomicMax(&misc[1], s_hi);
@@ -405,82 +522,63 @@ __global__ void zc_count(const xm_obj *__restrict__ objs, unsigned long long n, 
     }
 }
 
-// After the scan: bucket cursors bcur[b] = zone_off[b << shift], zones above
-// kWarpZone listed for the block sort, largest zone in misc[4], dropped count
-// stored beside the offsets (zone_off[n_zones + 1]).
-__global__ void zc_classify(const uint32_t *__restrict__ cnt, uint32_t *__restrict__ zone_off, int n_zones,
-                            int shift, uint32_t *__restrict__ bcur, uint32_t *__restrict__ big,
-                            uint32_t *__restrict__ misc)
+// Pass 2: every kept record into its bucket (unordered inside it) as a 32-byte
+// ZRec; bcur holds the buckets' start offsets and ends as their end offsets.
+// Records stream through shared memory (for_each_tile); each thread first
+// claims the slots of its 8 records (8 independent atomics in flight, one per
+// run of equal buckets in a warp), then writes them.
+__global__ void __launch_bounds__(kStageThreads, 2)
+zc_scatter(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp, int shift, bool bulk_ok,
+           uint32_t *__restrict__ bcur, ZRec *__restrict__ recs, uint32_t *__restrict__ misc)
 {
-    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z <= n_zones; z += gridDim.x * blockDim.x) {
-        if (z == n_zones) {
-            zone_off[n_zones + 1] = misc[2];
-            continue;
-        }
-        if ((z & ((1 << shift) - 1)) == 0) bcur[z >> shift] = zone_off[z];
-        const uint32_t m = cnt[z];
-        if (m > (uint32_t)kWarpZone) {
-            big[atomicAdd(&misc[3], 1u)] = (uint32_t)z;
-            atomicMax(&misc[4], m);
-        }
-    }
-}
-
-// Pass 2: every kept object's record into its bucket (unordered inside it).
-__global__ void zc_scatter(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp, int shift,
-                           uint32_t *__restrict__ bcur, ZRec *__restrict__ recs)
-{
+    extern __shared__ __align__(128) unsigned char scat_smem[];
+    TileRing &R = *reinterpret_cast<TileRing *>(scat_smem);
     const unsigned lane = threadIdx.x & 31;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x * kScatterU;
-    const unsigned long long warp0 =
-        (((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ull) * kScatterU;
-    for (unsigned long long wb = warp0; wb < n; wb += stride) {
-        int bk[kScatterU];
-        uint32_t zl[kScatterU];
-        xm_obj o[kScatterU];
+    const uint32_t zmask = (1u << shift) - 1u;
+    const bool ok = for_each_tile(objs, n, bulk_ok, R, [&](unsigned long long first, uint32_t cnt,
+                                                            const unsigned long long *w) {
+        uint32_t base[kPerThread];
+        unsigned head[kPerThread];
+        int zl[kPerThread];   // zone within the bucket, -1 = no record
 #pragma unroll
-        for (int u = 0; u < kScatterU; ++u) {
-            const unsigned long long i = wb + 32u * u + lane;
-            bk[u] = -2;
-            zl[u] = 0;
-            if (i < n) {
-                o[u] = objs[i];
-                const int z = isfinite(o[u].ra_deg) ? xm::zone_of(o[u].dec_deg, kp.zh_deg, kp.n_zones) : -1;
-                bk[u] = z < 0 ? -1 : (z >> shift);
-                zl[u] = (uint32_t)z & ((1u << shift) - 1u);
+        for (int u = 0; u < kPerThread; ++u) {
+            const uint32_t i = threadIdx.x + (uint32_t)u * kStageThreads;
+            int bk = -2;
+            zl[u] = -1;
+            if (i < cnt) {
+                const int z = rec_zone(rec_ra(w, i), rec_dec(w, i), kp);
+                bk = z < 0 ? -1 : (z >> shift);
+                if (z >= 0) zl[u] = (int)((uint32_t)z & zmask);
             }
-        }
-        uint32_t base[kScatterU];
-        unsigned head[kScatterU];
-#pragma unroll
-        for (int u = 0; u < kScatterU; ++u) {
-            const Run r = warp_run(bk[u], lane);
+            const Run r = warp_run(bk, lane);
             head[u] = r.head;
             base[u] = 0;
-            if (r.is_head && bk[u] >= 0) base[u] = atomicAdd(&bcur[bk[u]], r.len);
+            if (r.is_head && bk >= 0) base[u] = atomicAdd(&bcur[bk], r.len);
         }
 #pragma unroll
-        for (int u = 0; u < kScatterU; ++u) {
+        for (int u = 0; u < kPerThread; ++u) {
             const uint32_t b0 = __shfl_sync(0xffffffffu, base[u], head[u]);
-            if (bk[u] >= 0) {
-                const unsigned long long i = wb + 32u * u + lane;
-                const double ra = __ddiv_rn(o[u].ra_deg, XM_RAD2DEG);
-                const double dec = __ddiv_rn(o[u].dec_deg, XM_RAD2DEG);
+            if (zl[u] >= 0) {
+                const uint32_t i = threadIdx.x + (uint32_t)u * kStageThreads;
+                const double ra = __ddiv_rn(rec_ra(w, i), XM_RAD2DEG);
+                const double dec = __ddiv_rn(rec_dec(w, i), XM_RAD2DEG);
+                const unsigned long long id = w[3 * i];
                 ZRec *q = recs + b0 + (lane - head[u]);
                 reinterpret_cast<double2 *>(q)[0] = make_double2(ra, dec);
                 reinterpret_cast<uint4 *>(q)[1] =
-                    make_uint4((uint32_t)(unsigned long long)o[u].id, (uint32_t)((unsigned long long)o[u].id >> 32),
-                               zl[u] << kRaqBits | xm::raq32(ra) >> (32 - kRaqBits), (uint32_t)i);
+                    make_uint4((uint32_t)id, (uint32_t)(id >> 32),
+                               (uint32_t)zl[u] << kRaqBits | xm::raq32(ra) >> (32 - kRaqBits),
+                               (uint32_t)(first + i));
             }
         }
-    }
+    });
+    if (!ok && threadIdx.x == 0) atomicOr(&misc[5], 2u);
 }
 
 struct ZOut {
     long long *id;
     double2 *radec;
     float4 *xyz;
-    double *xyz64;
 };
 
 __device__ __forceinline__ ZRec zs_load(const ZRec *p)
@@ -504,24 +602,28 @@ __device__ __forceinline__ void zs_emit(const ZRec &r, unsigned long long j, con
     o.radec[j] = make_double2(r.ra, r.dec);
     o.xyz[j] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z),
                            __uint_as_float(r.raq & kRaqMask));
-    o.xyz64[3 * j] = x;
-    o.xyz64[3 * j + 1] = y;
-    o.xyz64[3 * j + 2] = z;
+}
+
+// Sort key of a record inside its zone: (raq, input index).
+__device__ __forceinline__ unsigned long long zrec_key(const ZRec *p)
+{
+    const uint4 t = reinterpret_cast<const uint4 *>(p)[1];
+    return ((unsigned long long)(t.z & kRaqMask) << 32) | t.w;
 }
 
 // Per-warp scratch of the in-zone sort.
 struct WarpSort {
-    unsigned long long key[kWarpZone];   // (raq << 32 | idx), grouped by sub-range
-    uint16_t at[kWarpZone];              // record at each rank
+    unsigned long long key[kWarpZone];   // keys grouped by raq sub-range
+    uint16_t at[kWarpZone];              // zone entry at each rank
     uint32_t cnt[32], base[32];
 };
 
-// Sorts the m <= kWarpZone records zr[0..m) by (raq, idx) and writes them to
-// the outputs from position j0.  Keys are grouped by the top 5 raq bits
-// (32 sub-ranges of the turn), then ranked inside their group.
-template <int E>
-__device__ __forceinline__ void zs_sort_zone(const ZRec *zr, uint32_t m, unsigned long long j0, WarpSort &W,
-                                             unsigned lane, const ZOut &o)
+// Ranks the m <= kWarpZone keys key_of(0..m) of one zone by value (distinct:
+// the input index is part of the key): W.at[rank] = entry.  Keys are grouped
+// by the top 5 raq bits (32 sub-ranges of the turn), then ranked inside their
+// group.
+template <int E, class K>
+__device__ __forceinline__ void zs_rank_zone(uint32_t m, K key_of, WarpSort &W, unsigned lane)
 {
     W.cnt[lane] = 0;
     __syncwarp();
@@ -534,10 +636,8 @@ __device__ __forceinline__ void zs_sort_zone(const ZRec *zr, uint32_t m, unsigne
         sub[e] = 0;
         slot[e] = 0;
         if (k < m) {
-            const uint4 t = reinterpret_cast<const uint4 *>(zr + k)[1];
-            const uint32_t raq = t.z & kRaqMask;
-            key[e] = ((unsigned long long)raq << 32) | t.w;
-            sub[e] = raq >> (kRaqBits - 5);
+            key[e] = key_of(k);
+            sub[e] = (uint32_t)(key[e] >> (32 + kRaqBits - 5));
             slot[e] = atomicAdd(&W.cnt[sub[e]], 1u);
         }
     }
@@ -554,10 +654,7 @@ __device__ __forceinline__ void zs_sort_zone(const ZRec *zr, uint32_t m, unsigne
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const uint32_t k = lane + 32u * e;
-        if (k < m) {
-            const uint32_t p = W.base[sub[e]] + slot[e];
-            W.key[p] = key[e];
-        }
+        if (k < m) W.key[W.base[sub[e]] + slot[e]] = key[e];
     }
     __syncwarp();
     uint32_t rank[E];
@@ -579,57 +676,128 @@ __device__ __forceinline__ void zs_sort_zone(const ZRec *zr, uint32_t m, unsigne
         if (k < m) W.at[rank[e]] = (uint16_t)k;
     }
     __syncwarp();
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const uint32_t p = lane + 32u * e;
-        if (p < m) zs_emit(zs_load(zr + W.at[p]), j0 + p, o);
-    }
-    __syncwarp();
 }
 
-// One block per bucket: records into zone order inside the bucket (recs_z),
-// then the zones of at most kWarpZone objects sorted and written out.
-__global__ void __launch_bounds__(kBucketThreads)
-zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint32_t *__restrict__ zone_off,
-          int n_zones, int shift, int n_buckets, KeyParams kp, ZOut o, uint32_t *__restrict__ misc)
+template <class K>
+__device__ __forceinline__ void zs_rank(uint32_t m, K key_of, WarpSort &W, unsigned lane)
 {
-    constexpr int kW = kBucketThreads / 32;
-    __shared__ uint32_t cur[1 << kBucketMaxShift];
-    __shared__ WarpSort ws[kW];
+    if (m <= 32) zs_rank_zone<1>(m, key_of, W, lane);
+    else if (m <= 64) zs_rank_zone<2>(m, key_of, W, lane);
+    else if (m <= 128) zs_rank_zone<4>(m, key_of, W, lane);
+    else zs_rank_zone<8>(m, key_of, W, lane);
+}
+
+// Pass 3, one block per bucket (buckets blockIdx.x, + gridDim.x, ...):
+//  1. the bucket's (raq, index) keys and record positions into shared memory
+//     in zone order (zone counts, their scan, shared-memory cursors);
+//  2. the zone offsets of the bucket's zones (zone_off);
+//  3. each zone of at most kWarpZone objects ranked by one warp and written out
+//     as the segment's SoA, its records gathered from the bucket (read a second
+//     time, from L2); larger zones are copied in zone order to recs_z and
+//     listed for zs_block.
+// A bucket of more than kBucketCap records orders its records through recs_z in
+// global memory instead of shared memory.
+constexpr int kBucketCap = 6144;
+constexpr int kBucketWarps = kBucketThreads / 32;
+
+struct BucketSmem {
+    unsigned long long key[kBucketCap];
+    uint16_t pos[kBucketCap];
+    uint32_t zcnt[1 << kBucketMaxShift];
+    uint32_t zbeg[(1 << kBucketMaxShift) + 1];
+    uint32_t zcur[1 << kBucketMaxShift];
+    WarpSort ws[kBucketWarps];
+};
+
+__global__ void __launch_bounds__(kBucketThreads, 2)
+zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint32_t *__restrict__ bend,
+          uint32_t *__restrict__ zone_off, int n_zones, int shift, int n_buckets, ZOut o,
+          uint32_t *__restrict__ big, uint32_t *__restrict__ misc)
+{
+    extern __shared__ __align__(16) unsigned char bk_smem[];
+    BucketSmem &S = *reinterpret_cast<BucketSmem *>(bk_smem);
     const unsigned lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    WarpSort &W = S.ws[warp];
     for (int bk = blockIdx.x; bk < n_buckets; bk += gridDim.x) {
         const int z0 = bk << shift;
         const int nzb = min(1 << shift, n_zones - z0);
-        const uint32_t r0 = zone_off[z0], r1 = zone_off[z0 + nzb];
-        if (threadIdx.x < nzb) cur[threadIdx.x] = zone_off[z0 + threadIdx.x];
+        const uint32_t r0 = bk ? bend[bk - 1] : 0u, r1 = bend[bk];
+        const uint32_t m = r1 - r0;
+        if (threadIdx.x < 32) S.zcnt[threadIdx.x] = 0;
         __syncthreads();
-        if (nzb == 1) {
-            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) recs_z[i] = recs_b[i];
-        } else {
-            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                const double2 a = reinterpret_cast<const double2 *>(recs_b + i)[0];
-                const uint4 t = reinterpret_cast<const uint4 *>(recs_b + i)[1];
-                const uint32_t zl = t.z >> kRaqBits;
-                if (zl >= (uint32_t)nzb) {   // cannot happen: written by zc_scatter for this bucket
-                    atomicOr(&misc[5], 1u);
-                    continue;
+        // zone counts
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+            const uint32_t zl = reinterpret_cast<const uint4 *>(recs_b + r0 + i)[1].z >> kRaqBits;
+            if (zl < (uint32_t)nzb) atomicAdd(&S.zcnt[zl], 1u);
+            else atomicOr(&misc[5], 1u);   // cannot happen: written by zc_scatter for this bucket
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {   // exclusive scan of the (at most 32) zone counts
+            const uint32_t c = (int)threadIdx.x < nzb ? S.zcnt[threadIdx.x] : 0u;
+            uint32_t incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= (unsigned)d) incl += y;
+            }
+            S.zbeg[threadIdx.x] = incl - c;
+            S.zcur[threadIdx.x] = incl - c;
+            if (threadIdx.x == 31) S.zbeg[32] = incl;
+            if ((int)threadIdx.x < nzb) {
+                zone_off[z0 + threadIdx.x] = r0 + incl - c;
+                if (c > (uint32_t)kWarpZone) {
+                    big[atomicAdd(&misc[3], 1u)] = (uint32_t)(z0 + threadIdx.x);
+                    atomicMax(&misc[4], c);
                 }
-                const uint32_t p = atomicAdd(&cur[zl], 1u);
-                reinterpret_cast<double2 *>(recs_z + p)[0] = a;
-                reinterpret_cast<uint4 *>(recs_z + p)[1] = t;
+            }
+            if (bk == n_buckets - 1 && threadIdx.x == 0) {
+                zone_off[n_zones] = r1;
+                zone_off[n_zones + 1] = misc[2];
             }
         }
         __syncthreads();
-        for (int k = warp; k < nzb; k += kW) {
-            const uint32_t b = zone_off[z0 + k];
-            const uint32_t m = zone_off[z0 + k + 1] - b;
-            if (m == 0 || m > (uint32_t)kWarpZone) continue;
-            const ZRec *zr = recs_z + b;
-            if (m <= 32) zs_sort_zone<1>(zr, m, b, ws[warp], lane, o);
-            else if (m <= 64) zs_sort_zone<2>(zr, m, b, ws[warp], lane, o);
-            else if (m <= 128) zs_sort_zone<4>(zr, m, b, ws[warp], lane, o);
-            else zs_sort_zone<8>(zr, m, b, ws[warp], lane, o);
+        const bool in_smem = m <= (uint32_t)kBucketCap;
+        // keys (and positions) in zone order
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+            const ZRec *p = recs_b + r0 + i;
+            const uint4 t = reinterpret_cast<const uint4 *>(p)[1];
+            const uint32_t zl = t.z >> kRaqBits;
+            if (zl >= (uint32_t)nzb) continue;
+            const uint32_t q = atomicAdd(&S.zcur[zl], 1u);
+            if (in_smem) {
+                S.key[q] = ((unsigned long long)(t.z & kRaqMask) << 32) | t.w;
+                S.pos[q] = (uint16_t)i;
+            } else {
+                const double2 a = reinterpret_cast<const double2 *>(p)[0];
+                reinterpret_cast<double2 *>(recs_z + r0 + q)[0] = a;
+                reinterpret_cast<uint4 *>(recs_z + r0 + q)[1] = t;
+            }
+        }
+        __syncthreads();
+        for (int k = warp; k < nzb; k += kBucketWarps) {
+            const uint32_t zb = S.zbeg[k], mz = S.zbeg[k + 1] - zb;
+            if (mz == 0) continue;
+            if (mz > (uint32_t)kWarpZone) {   // zs_block sorts it from recs_z
+                if (in_smem)
+                    for (uint32_t q = lane; q < mz; q += 32) {
+                        const ZRec *p = recs_b + r0 + S.pos[zb + q];
+                        reinterpret_cast<double2 *>(recs_z + r0 + zb + q)[0] = reinterpret_cast<const double2 *>(p)[0];
+                        reinterpret_cast<uint4 *>(recs_z + r0 + zb + q)[1] = reinterpret_cast<const uint4 *>(p)[1];
+                    }
+                continue;
+            }
+            if (in_smem) {
+                zs_rank(mz, [&](uint32_t q) { return S.key[zb + q]; }, W, lane);
+                for (uint32_t p = lane; p < mz; p += 32)
+                    zs_emit(zs_load(recs_b + r0 + S.pos[zb + W.at[p]]), (unsigned long long)r0 + zb + p, o);
+            } else {
+                const ZRec *zr = recs_z + r0 + zb;
+                zs_rank(mz, [&](uint32_t q) { return zrec_key(zr + q); }, W, lane);
+                for (uint32_t p = lane; p < mz; p += 32)
+                    zs_emit(zs_load(zr + W.at[p]), (unsigned long long)r0 + zb + p, o);
+            }
+            __syncwarp();
         }
         __syncthreads();
     }
@@ -810,7 +978,7 @@ static xm_status build_lsd(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_s
         const unsigned long long mask = (1ull << raq_bits) - 1;
         zb_gather<<<grid_for(seg->n, 256, ctx->sm_count, 8), 256, 0, st>>>(kin, vin, objs, seg->n, mask,
                                                                             (long long *)seg->id, seg->radec,
-                                                                            seg->xyz, seg->xyz64);
+                                                                            seg->xyz);
         launches++;
     }
     XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0xFF, ((size_t)nz + 1) * 4, st));
@@ -845,25 +1013,36 @@ static xm_status build_lsd(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_s
 
 // The segment's arrays live in one allocation (fewer, equal-sized blocks keep
 // the context's memory pool from fragmenting when segments come and go):
-// zone_off, id, radec, xyz, xyz64, each 256-byte aligned.
+// zone_off, id, radec, xyz, each 256-byte aligned.
+void xm_seg_layout(xm_segment *seg, void *base)
+{
+    char *w = (char *)base;
+    seg->zone_off = base ? (uint32_t *)w : nullptr;
+    seg->id = base ? (int64_t *)(w + seg->off_id) : nullptr;
+    seg->radec = base ? (double2 *)(w + seg->off_radec) : nullptr;
+    seg->xyz = base ? (float4 *)(w + seg->off_xyz) : nullptr;
+}
+
 xm_status xm_seg_storage(xm_segment *seg, uint64_t n)
 {
     xm_ctx *ctx = seg->ctx;
+    if (seg->host_store) {   // a rebuild makes the host copy of an offloaded segment stale
+        cudaFreeHost(seg->host_store);
+        seg->host_store = nullptr;
+    }
     if (seg->store && seg->cap >= n) return XM_OK;
     const uint64_t c = std::max<uint64_t>(n, 1);
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t bz = al(((size_t)seg->n_zones + 8) * 4), bi = al((c + 2) * 8), br = al(c * 16), bx = al(c * 16),
-                 b6 = al((c + 2) * 24);
+    const size_t bz = al(((size_t)seg->n_zones + 8) * 4), bi = al((c + 2) * 8), br = al(c * 16), bx = al(c * 16);
     xm_dev_free(ctx, seg->store);
     seg->store = nullptr;
     seg->cap = 0;
-    XM_TRY(xm_dev_alloc(ctx, &seg->store, bz + bi + br + bx + b6));
-    char *w = (char *)seg->store;
-    seg->zone_off = (uint32_t *)w; w += bz;
-    seg->id = (int64_t *)w; w += bi;
-    seg->radec = (double2 *)w; w += br;
-    seg->xyz = (float4 *)w; w += bx;
-    seg->xyz64 = (double *)w;
+    XM_TRY(xm_dev_alloc(ctx, &seg->store, bz + bi + br + bx));
+    seg->store_bytes = bz + bi + br + bx;
+    seg->off_id = bz;
+    seg->off_radec = bz + bi;
+    seg->off_xyz = bz + bi + br;
+    xm_seg_layout(seg, seg->store);
     seg->cap = c;
     XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0, bz, ctx->stream));
     return XM_OK;
@@ -881,72 +1060,84 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     xm_raq_layout(nz, &raq_bits, &passes);
     seg->raq_bits = raq_bits;
     XM_TRY(xm_seg_storage(seg, n));
-    const uint64_t nn = std::max<uint64_t>(n, 1);
+    seg->n_in = n;
+    if (n == 0) {   // every zone empty
+        XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0, ((size_t)nz + 2) * 4, st));
+        XM_CUDA(ctx, cudaStreamSynchronize(st));
+        seg->n = 0;
+        seg->dropped_host = 0;
+        seg->z_lo = 0;
+        seg->z_hi = -1;
+        return XM_OK;
+    }
     // buckets of 2^shift zones, at least 4 per SM
     int shift = kBucketMaxShift;
     while (shift > 0 && (nz >> shift) < ctx->sm_count * 4) --shift;
     const int n_buckets = (nz + (1 << shift) - 1) >> shift;
-    // scratch: records by bucket and by zone, per-zone counts, bucket cursors,
-    // big-zone list, scan scratch, misc
-    const size_t rb = (nn * sizeof(ZRec) + 255) & ~(size_t)255;
-    const size_t zb = (((size_t)nz + 1) * 4 + 255) & ~(size_t)255;
+    // scratch: records by bucket, records of large zones in zone order, bucket
+    // counts and cursors, large-zone list, scan scratch, misc
+    const size_t rb = (n * sizeof(ZRec) + 255) & ~(size_t)255;
     const size_t bb = (((size_t)n_buckets + 1) * 4 + 255) & ~(size_t)255;
-    const size_t sb = (xm_scan_tmp_bytes((size_t)nz) + 255) & ~(size_t)255;
+    const size_t zb = (((size_t)nz + 1) * 4 + 255) & ~(size_t)255;
+    const size_t sb = (xm_scan_tmp_bytes((size_t)n_buckets) + 255) & ~(size_t)255;
     const size_t mb = 256;
-    XM_TRY(ensure(ctx, &ctx->build_tmp, &ctx->build_tmp_bytes, 2 * rb + 2 * zb + bb + sb + mb));
+    XM_TRY(ensure(ctx, &ctx->build_tmp, &ctx->build_tmp_bytes, 2 * rb + 2 * bb + zb + sb + mb));
     char *w = (char *)ctx->build_tmp;
     ZRec *recs_b = (ZRec *)w; w += rb;
     ZRec *recs_z = (ZRec *)w; w += rb;
-    uint32_t *cnt = (uint32_t *)w; w += zb;
-    uint32_t *big = (uint32_t *)w; w += zb;
+    uint32_t *bcnt = (uint32_t *)w; w += bb;
     uint32_t *bcur = (uint32_t *)w; w += bb;
+    uint32_t *big = (uint32_t *)w; w += zb;
     void *scan_tmp = w; w += sb;
-    uint32_t *misc = (uint32_t *)w;   // z_lo, z_hi, dropped, n_big, largest zone, error
+    uint32_t *misc = (uint32_t *)w;   // z_lo, z_hi, dropped, n_big, largest big zone, error bits
     uint32_t launches = 0;
+    static bool attr = false;
+    const size_t smem_scatter = sizeof(TileRing), smem_bucket = sizeof(BucketSmem);
+    const size_t smem_block = (size_t)kBlockZone * 10;
+    if (!attr) {
+        XM_CUDA(ctx, cudaFuncSetAttribute(zc_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kHistMax * 4));
+        XM_CUDA(ctx, cudaFuncSetAttribute(zc_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_scatter));
+        XM_CUDA(ctx, cudaFuncSetAttribute(zs_bucket, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bucket));
+        XM_CUDA(ctx, cudaFuncSetAttribute(zs_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_block));
+        attr = true;
+    }
 
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[0], st));
-    XM_CUDA(ctx, cudaMemsetAsync(cnt, 0, (size_t)nz * 4, st));
+    XM_CUDA(ctx, cudaMemsetAsync(bcnt, 0, (size_t)n_buckets * 4, st));
     XM_CUDA(ctx, cudaMemsetAsync(misc, 0, 32, st));
     XM_CUDA(ctx, cudaMemsetAsync(misc, 0xFF, 4, st));
     KeyParams kp{seg->zh_deg, nz, 32 - raq_bits, raq_bits, passes};
-    if (n > 0) {
-        zc_count<<<grid_for((n + kScatterU - 1) / kScatterU, 256, ctx->sm_count, 8), 256, 0, st>>>(objs, n, kp, cnt,
-                                                                                                   misc);
-        launches++;
-    }
+    const uint64_t cgroups = (n + kCountU - 1) / kCountU;
+    if (n_buckets <= kHistMax)
+        zc_count<true><<<grid_for(cgroups, 256, ctx->sm_count, 2), 256, (size_t)n_buckets * 4, st>>>(
+            objs, n, kp, shift, n_buckets, bcnt, misc);
+    else
+        zc_count<false><<<grid_for(cgroups, 256, ctx->sm_count, 8), 256, 0, st>>>(objs, n, kp, shift, n_buckets,
+                                                                                  bcnt, misc);
+    launches++;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[8], st));
-    XM_CUDA(ctx, xm_scan_exclusive_u32(cnt, seg->zone_off, (size_t)nz, scan_tmp, st));
-    zc_classify<<<grid_for((uint64_t)nz + 1, 256, ctx->sm_count, 8), 256, 0, st>>>(cnt, seg->zone_off, nz, shift,
-                                                                                     bcur, big, misc);
-    launches += 4;
+    XM_CUDA(ctx, xm_scan_exclusive_u32(bcnt, bcur, (size_t)n_buckets, scan_tmp, st));
+    launches += 3;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[9], st));
-    if (n > 0) {
-        zc_scatter<<<grid_for((n + kScatterU - 1) / kScatterU, 256, ctx->sm_count, 8), 256, 0, st>>>(
-            objs, n, kp, shift, bcur, recs_b);
-        launches++;
-    }
+    const bool bulk_ok = ((uintptr_t)objs & 15) == 0;
+    const uint64_t n_tiles = (n + kTileRecs - 1) / kTileRecs;
+    zc_scatter<<<(unsigned)std::min<uint64_t>(n_tiles, (uint64_t)ctx->sm_count * 2), kStageThreads, smem_scatter,
+                 st>>>(objs, n, kp, shift, bulk_ok, bcur, recs_b, misc);
+    launches++;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[10], st));
-    ZOut o{(long long *)seg->id, seg->radec, seg->xyz, seg->xyz64};
-    if (n > 0) {
-        zs_bucket<<<std::min(n_buckets, ctx->sm_count * 8), kBucketThreads, 0, st>>>(
-            recs_b, recs_z, seg->zone_off, nz, shift, n_buckets, kp, o, misc);
-        static bool attr = false;
-        const size_t smem = (size_t)kBlockZone * 10;
-        if (!attr) {
-            XM_CUDA(ctx, cudaFuncSetAttribute(zs_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            attr = true;
-        }
-        zs_block<<<ctx->sm_count * 2, kZsThreads, smem, st>>>(recs_z, seg->zone_off, big, misc, o);
-        launches += 2;
-    }
+    ZOut o{(long long *)seg->id, seg->radec, seg->xyz};
+    zs_bucket<<<std::min(n_buckets, ctx->sm_count * 2), kBucketThreads, smem_bucket, st>>>(
+        recs_b, recs_z, bcur, seg->zone_off, nz, shift, n_buckets, o, big, misc);
+    zs_block<<<ctx->sm_count * 2, kZsThreads, smem_block, st>>>(recs_z, seg->zone_off, big, misc, o);
+    launches += 2;
     XM_CUDA(ctx, cudaGetLastError());
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[11], st));
     uint32_t hm[8];
     XM_CUDA(ctx, cudaMemcpyAsync(hm, misc, 32, cudaMemcpyDeviceToHost, st));
     XM_CUDA(ctx, cudaStreamSynchronize(st));
-    const uint64_t dropped = n ? hm[2] : 0;
+    const uint64_t dropped = hm[2];
     seg->n = n - dropped;
-    seg->n_in = n;
     seg->dropped_host = (uint32_t)dropped;
     if (seg->n > 0) {
         seg->z_lo = (int32_t)hm[0];
@@ -955,9 +1146,13 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
         seg->z_lo = 0;
         seg->z_hi = -1;
     }
-    if (hm[5]) {
+    if (hm[5] & 1u) {
         ctx->last_error = "zone build: a record left its bucket";
         return XM_ERR_CUDA;
+    }
+    if (hm[5] & 2u) {
+        ctx->last_error = "zone build: a bounded wait for a bulk copy of records ran out";
+        return XM_ERR_TIMEOUT;
     }
     if (hm[4] > (uint32_t)kBlockZone) *fallback = true;
     if (stats) {
@@ -966,10 +1161,10 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
         cudaEventElapsedTime(&b, ctx->ev[8], ctx->ev[9]);
         cudaEventElapsedTime(&c, ctx->ev[9], ctx->ev[10]);
         cudaEventElapsedTime(&d, ctx->ev[10], ctx->ev[11]);
-        stats->ms_zb_count += a;    // objects per zone
-        stats->ms_zb_scan += b;     // zone offsets
-        stats->ms_zb_scatter += c;  // records into zone buckets
-        stats->ms_zb_sort += d;     // in-zone sort + SoA output
+        stats->ms_zb_count += a;    // objects per bucket
+        stats->ms_zb_scan += b;     // bucket offsets
+        stats->ms_zb_scatter += c;  // records into buckets
+        stats->ms_zb_sort += d;     // zone offsets, in-zone sort + SoA output
         stats->ms_build += a + b + c + d;
         stats->n_launches += launches;
     }
@@ -1112,7 +1307,7 @@ extern "C" xm_status xm_segment_build_noalloc(int device, void *stream, const xm
     if (kept > 0)
         zb_gather<<<grid_for(kept, 256, sm_count, 8), 256, 0, st>>>(kin, vin, objs, kept, (1ull << raq_bits) - 1,
                                                                     (long long *)out_id, (double2 *)out_radec,
-                                                                    (float4 *)out_xyz, nullptr);
+                                                                    (float4 *)out_xyz);
     if (cudaMemsetAsync(out_zone_off, 0xFF, ((size_t)nz + 1) * 4, st) != cudaSuccess) return XM_ERR_CUDA;
     if (n > 0) zb_bounds_mark<<<grid_for(n, 256, sm_count, 8), 256, 0, st>>>(kin, n, raq_bits, nz, out_zone_off);
     zb_bounds_fill<<<grid_for((uint64_t)nz + 1, 256, sm_count, 8), 256, 0, st>>>(kin, n, raq_bits, nz, out_zone_off);

@@ -4,15 +4,24 @@
 //   xmatch [-r arcsec] [-z arcsec] [-n objects] [-t gpus] [-m maxout]
 //          [-o outdir] [-x] [-v [level]] [--dist] fileA fileB
 //
-// fileA (the smaller file) is cut into segments of -n objects, zone-built on
-// every GPU used and kept resident; fileB is read in rounds of one segment per
-// GPU.  On each GPU a worker thread matches every resident A segment against
-// its B segment in one batch launch and writes the pairs of the round to
+// fileA (the file held in memory; pass the smaller one first) is cut into
+// segments of -n objects and zone-built on every GPU used; fileB is read in
+// rounds of one segment per GPU.  On each GPU a worker thread matches every A
+// segment against its B segment and writes the pairs of the round to
 // outdir/<wid> (wid counts workers over rounds, as BoostXmatch.cpp:312-320),
 // 16-byte {idA, idB} records as Worker.cu:413-417 (--dist: 24-byte records
 // with the distance in radians).  While a round is matched, the worker's
 // second context reads and zone-builds its next B segment, so file reads,
 // host-to-device copies and builds overlap the matching.
+//
+// A's segments stay in device memory when they fit --resident-mb (default:
+// 60 % of the GPU's free memory); the round is then one batch launch of all
+// of them.  Otherwise, as the reference does with its host-resident segments
+// (BoostXmatch.cpp:247-274, Worker.cu:251-292), they are kept in pinned host
+// memory and paged in one job at a time, the next A segment's copy
+// overlapping the current match; rounds alternate the order of the A segments
+// so that the last one of a round is still on the device for the first job of
+// the next (the reference's job affinity, JobManager.cpp:16-41).
 //
 // Differences: the output directory must not exist unless -x is given (the
 // reference asks on the terminal); -m caps the pairs written per job and
@@ -21,6 +30,7 @@
 #include <sys/stat.h>
 
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -36,6 +46,7 @@ namespace {
 struct Options {
     double r_arcsec = 5, zh_arcsec = 0;
     uint64_t numobj = 0, maxout = 0;
+    double resident_mb = -1;   // device MiB for fileA's segments; < 0 = 60 % of the free memory
     uint32_t threads = 0;
     int verbose = 0;
     bool overwrite = false, dist = false;
@@ -56,8 +67,10 @@ void usage(FILE *f)
                  "  -x, --overwrite          allow an existing output directory\n"
                  "  -v, --verbose [LEVEL]    progress on stderr\n"
                  "      --dist               24-byte records {idA, idB, distance}\n"
+                 "      --resident-mb MIB    device memory fileA's segments may hold (default: 60%% of the\n"
+                 "                           free memory); beyond it they are paged in from host memory per job\n"
                  "  -h, --help\n"
-                 "fileA is held in device memory, fileB is looped over.\n");
+                 "fileA is held in memory (pass the smaller file first), fileB is looped over.\n");
 }
 
 bool parse(int argc, char **argv, Options &o, int &rc)
@@ -100,6 +113,9 @@ bool parse(int argc, char **argv, Options &o, int &rc)
             o.overwrite = true;
         } else if (a == "--dist") {
             o.dist = true;
+        } else if (a == "--resident-mb") {
+            if (!(v = value(i, "--resident-mb"))) break;
+            o.resident_mb = std::atof(v);
         } else if (a == "-v" || a == "--verbose") {
             o.verbose = 9;
             if (i + 1 < argc && argv[i + 1][0] >= '0' && argv[i + 1][0] <= '9') o.verbose = std::atoi(argv[++i]);
@@ -167,7 +183,9 @@ int main(int argc, char **argv)
     uint64_t na = 0, nb = 0;
     if (!check(xm_idradec_count(fa.c_str(), &na), fa.c_str()) || !check(xm_idradec_count(fb.c_str(), &nb), fb.c_str()))
         return 1;
-    if (nb < na) std::fprintf(stderr, "xmatch: warning: the larger file is held in memory (%s)\n", fa.c_str());
+    if (nb < na)
+        std::fprintf(stderr, "xmatch: warning: fileA (%s) is the larger file; it is the one held in memory, pass "
+                     "the smaller file first to hold less\n", fa.c_str());
     const uint64_t seg_a = o.numobj ? o.numobj : std::max<uint64_t>(na, 1);
     const uint64_t seg_b = o.numobj ? o.numobj : std::max<uint64_t>(nb, 1);
     if (!o.outdir.empty()) {
@@ -203,7 +221,14 @@ int main(int argc, char **argv)
     }
     const uint32_t T = (uint32_t)W.size();
     const double t0 = now_s();
-    // A: all segments, resident on every GPU (BoostXmatch.cpp:246-272)
+    // A: all segments on every GPU (BoostXmatch.cpp:246-272), in device memory
+    // when they fit the budget, else in pinned host memory
+    uint64_t free_b = 0;
+    xm_ctx_info(W[0].mctx, nullptr, nullptr, &free_b, nullptr);
+    const double budget = o.resident_mb >= 0 ? o.resident_mb * 1048576.0 : 0.6 * (double)free_b;
+    const uint64_t n_aseg = na ? (na + seg_a - 1) / seg_a : 1;
+    const double a_bytes = 40.0 * (double)na + 4.0 * (std::ceil(180 / zh_deg) + 8) * (double)n_aseg;
+    const bool paged = a_bytes > budget;
     uint32_t sid = 0;
     for (uint64_t first = 0; first < na || (na == 0 && first == 0); first += seg_a) {
         const uint64_t n = std::min<uint64_t>(seg_a, na - first);
@@ -211,14 +236,16 @@ int main(int argc, char **argv)
             xm_segment *s = nullptr;
             if (!check(load_segment(w.mctx, fa, first, n, sid, zh_deg, &s), "building a segment of fileA", w.mctx))
                 return 1;
+            if (paged && !check(xm_segment_offload(s), "moving a segment of fileA to host memory", w.mctx)) return 1;
             w.A.push_back(s);
         }
         ++sid;
         if (na == 0) break;
     }
     if (o.verbose)
-        std::fprintf(stderr, "xmatch: %s: %zu segment(s) of at most %llu objects on %u GPU(s), %.3f s\n", fa.c_str(),
-                     W[0].A.size(), (unsigned long long)seg_a, T, now_s() - t0);
+        std::fprintf(stderr, "xmatch: %s: %zu segment(s) of at most %llu objects on %u GPU(s) (%s), %.3f s\n",
+                     fa.c_str(), W[0].A.size(), (unsigned long long)seg_a, T,
+                     paged ? "in host memory, paged in per job" : "resident in device memory", now_s() - t0);
     // B: rounds of one segment per GPU (BoostXmatch.cpp:278-327)
     const uint64_t n_bseg = nb ? (nb + seg_b - 1) / seg_b : 0;
     const uint64_t rounds = (n_bseg + T - 1) / T;
@@ -242,50 +269,69 @@ int main(int argc, char **argv)
             }
             xm_segment *B = got.second;
             if (k + T < n_bseg) next = std::async(std::launch::async, build, k + T);
-            std::vector<xm_job> jobs;
-            for (xm_segment *a : w.A) jobs.push_back({a, B, r_deg});
-            std::vector<uint64_t> cnt(jobs.size());
-            xm_status st = xm_match_batch(w.mctx, jobs.data(), (uint32_t)jobs.size(),
-                                          o.dist ? XM_FILTER32 : XM_FILTER32 | XM_NO_DIST, nullptr, nullptr,
-                                          cnt.data(), nullptr);
-            if (!check(st, "matching", w.mctx)) {
-                w.rc = 1;
-                return;
-            }
+            const std::string path = o.outdir.empty() ? std::string() : o.outdir + "/" + std::to_string(round * T + g);
+            bool first_write = true;
             uint64_t total = 0;
-            for (uint64_t c : cnt) total += c;
-            // the batch's matches stay on the device grouped by job; one copy brings them over
-            std::vector<int64_t> pairs(2 * std::max<uint64_t>(total, 1));
-            std::vector<double> dist(o.dist ? std::max<uint64_t>(total, 1) : 0);
-            xm_pairs all = {pairs.data(), o.dist ? dist.data() : nullptr, total, 0};
-            if (total && !check(xm_fetch_pairs(w.mctx, &all), "fetching matches", w.mctx)) {
-                w.rc = 1;
-                return;
-            }
-            std::vector<xm_pairs> outs(jobs.size());
-            uint64_t off = 0;
-            for (size_t j = 0; j < jobs.size(); ++j) {
-                outs[j] = {pairs.data() + 2 * off, o.dist ? dist.data() + off : nullptr, cnt[j], cnt[j]};
-                off += cnt[j];
-            }
-            w.matches += total;
-            if (!o.outdir.empty()) {
-                const std::string path = o.outdir + "/" + std::to_string(round * T + g);
-                bool first = true;
+            // one batch launch of the given A segments against B; pairs appended to the round's file
+            auto run = [&](const std::vector<size_t> &aseg) -> bool {
+                std::vector<xm_job> jobs;
+                for (size_t a : aseg) jobs.push_back({w.A[a], B, r_deg});
+                std::vector<uint64_t> cnt(jobs.size());
+                xm_status st = xm_match_batch(w.mctx, jobs.data(), (uint32_t)jobs.size(),
+                                              o.dist ? XM_FILTER32 : XM_FILTER32 | XM_NO_DIST, nullptr, nullptr,
+                                              cnt.data(), nullptr);
+                if (!check(st, "matching", w.mctx)) return false;
+                uint64_t n_b = 0;
+                for (uint64_t c : cnt) n_b += c;
+                // the batch's matches stay on the device grouped by job; one copy brings them over
+                std::vector<int64_t> pairs(2 * std::max<uint64_t>(n_b, 1));
+                std::vector<double> dist(o.dist ? std::max<uint64_t>(n_b, 1) : 0);
+                xm_pairs all = {pairs.data(), o.dist ? dist.data() : nullptr, n_b, 0};
+                if (n_b && !check(xm_fetch_pairs(w.mctx, &all), "fetching matches", w.mctx)) return false;
+                total += n_b;
+                if (path.empty()) return true;
+                uint64_t off = 0;
                 for (size_t j = 0; j < jobs.size(); ++j) {
-                    xm_pairs p = outs[j];
+                    xm_pairs p = {pairs.data() + 2 * off, o.dist ? dist.data() + off : nullptr, cnt[j], cnt[j]};
+                    off += cnt[j];
                     if (o.maxout && p.count > o.maxout) {
-                        std::fprintf(stderr, "xmatch: job (A %zu, B %llu): %llu pairs, %llu written (-m)\n", j,
-                                     (unsigned long long)k, (unsigned long long)p.count, (unsigned long long)o.maxout);
+                        std::fprintf(stderr, "xmatch: job (A %zu, B %llu): %llu pairs, %llu written (-m)\n",
+                                     aseg[j], (unsigned long long)k, (unsigned long long)p.count,
+                                     (unsigned long long)o.maxout);
                         p.count = o.maxout;
                     }
-                    if (!check(xm_pairs_write(path.c_str(), &p, o.dist ? 24 : 16, first ? 0 : 1), path.c_str())) {
-                        w.rc = 1;
-                        return;
-                    }
-                    first = false;
+                    if (!check(xm_pairs_write(path.c_str(), &p, o.dist ? 24 : 16, first_write ? 0 : 1),
+                               path.c_str()))
+                        return false;
+                    first_write = false;
+                }
+                return true;
+            };
+            const size_t S = w.A.size();
+            bool ok = true;
+            if (!paged) {
+                std::vector<size_t> all(S);
+                for (size_t a = 0; a < S; ++a) all[a] = a;
+                ok = run(all);
+            } else {
+                // one A segment at a time, the next one's page-in queued before the current match;
+                // odd rounds walk the A segments backwards, so the first job reuses the last one
+                std::vector<size_t> order(S);
+                for (size_t q = 0; q < S; ++q) order[q] = (round & 1) ? S - 1 - q : q;
+                ok = check(xm_segment_page_in(w.A[order[0]]), "paging in a segment of fileA", w.mctx);
+                for (size_t q = 0; ok && q < S; ++q) {
+                    if (q + 1 < S)
+                        ok = check(xm_segment_page_in(w.A[order[q + 1]]), "paging in a segment of fileA", w.mctx);
+                    ok = ok && run({order[q]});
+                    if (ok && q + 1 < S)
+                        ok = check(xm_segment_page_out(w.A[order[q]]), "paging out a segment of fileA", w.mctx);
                 }
             }
+            if (!ok) {
+                w.rc = 1;
+                return;
+            }
+            w.matches += total;
             xm_segment_free(B);
             if (o.verbose)
                 std::fprintf(stderr, "xmatch: GPU %d round %llu: %llu pairs\n", w.device, (unsigned long long)round,

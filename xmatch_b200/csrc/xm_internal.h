@@ -95,14 +95,20 @@ struct xm_segment {
     int32_t z_lo = 0, z_hi = -1;   // first / last zone holding an object
     int raq_bits = 32;             // leading bits of the quantised ra kept in xyz.w
     uint32_t dropped_host = 0;
-    void *store = nullptr;         // one allocation holding the arrays below
+    void *store = nullptr;         // one device allocation holding the arrays below (null when offloaded)
+    size_t store_bytes = 0;        // its size, and the offsets of id, radec, xyz in it
+    size_t off_id = 0, off_radec = 0, off_xyz = 0;
+    void *host_store = nullptr;    // pinned host copy of the store (xm_segment_offload)
+    cudaEvent_t ready = nullptr;   // recorded after a page-in copy (xm_segment_page_in)
+    bool ready_pending = false;    // work on ctx->stream must wait for `ready` first
     uint32_t *zone_off = nullptr;  // [n_zones + 8]; [n_zones + 1] = dropped count; the rest
                                    // pads 16-byte bulk copies of zone-offset slices
     int64_t *id = nullptr;
     double2 *radec = nullptr;      // radians
     float4 *xyz = nullptr;         // FP32 unit vector; w = quantised-ra bits
-    double *xyz64 = nullptr;       // FP64 unit vector (x, y, z) per object, 2 spare objects
 };
+// Points the segment's arrays into a store of its layout at base (null clears them).
+void xm_seg_layout(xm_segment *seg, void *base);
 // Allocates (or keeps, when large enough) the segment's arrays for n objects.
 xm_status xm_seg_storage(xm_segment *seg, uint64_t n);
 
@@ -124,6 +130,8 @@ xm_status xm_seg_storage(xm_segment *seg, uint64_t n);
 
 // ---- internal entry points shared between translation units ----
 xm_status xm_dev_alloc(xm_ctx *ctx, void **p, size_t bytes);
+// The same, stream-ordered on another stream of the context.
+xm_status xm_dev_alloc_on(xm_ctx *ctx, void **p, size_t bytes, cudaStream_t st);
 void xm_dev_free(xm_ctx *ctx, void *p);
 // Runs the pair kernel over the jobs; ctx->res holds the (ungrouped) matches.
 // direct (optional): pinned host buffers (device-accessible pointers) the pair

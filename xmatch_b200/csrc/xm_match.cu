@@ -35,8 +35,9 @@
 // of Worker.cu:118 fixed.  XM_FILTER32 evaluates chord^2 in FP32 from the
 // FP32 unit vectors first: above thr_hi the pair cannot match; below thr_lo
 // (zones with an RA cut) it matches and the cuts provably hold; in between,
-// and in full-ring zones, B's ra/dec and both FP64 unit vectors are read and
-// the FP64 predicate decides.  The bounds are derived in xm_make_params, so
+// and in full-ring zones, B's ra/dec is read, both FP64 unit vectors are
+// computed from the ra/dec of the pair (the builder's sincos, so the same bits
+// every time) and the FP64 predicate decides.  The bounds are derived in xm_make_params, so
 // the pair set is the FP64 one bit for bit.  XM_PLAIN64 applies the FP64
 // predicate with per-pair sincos to every candidate.
 //
@@ -53,6 +54,7 @@
 
 #include "xm_internal.h"
 
+#include "xm_async.cuh"
 #include "xm_match.cuh"
 #include "xm_math.cuh"
 
@@ -61,69 +63,12 @@ namespace xm {
 namespace {
 
 constexpr double kWinEps = 1e-12;  // window widening (radians), >> FP64 rounding of ra +- alpha
-constexpr unsigned kWaitLimit = 1u << 26;   // bounded mbarrier wait (iterations)
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
-}
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// ---- mbarrier + bulk copy (TMA, no multicast) ----
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void fence_mbar_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase)
-{
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return done != 0;
-}
-
-// Bounded wait for the phase; false if it did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
-{
-    for (unsigned it = 0; it < kWaitLimit; ++it)
-        if (mbar_try_wait(bar, phase)) return true;
-    return false;
 }
 
 // ---- bisection on the quantised ra (xyz.w) ----
@@ -179,17 +124,27 @@ __device__ __forceinline__ Win make_win(double ra, double alpha, int shift)
     return w;
 }
 
+// FP64 chord^2 of two positions from their unit vectors, computed as the zone
+// builder computes them (the same bits).  Out of line: it runs for the few
+// pairs inside the FP32 margin band (and for distances), and keeping its
+// registers out of the pair loop keeps the loop's occupancy.
+__device__ __noinline__ double chord2_radec(double ra1, double dec1, double ra2, double dec2)
+{
+    double x1, y1, z1, x2, y2, z2;
+    radec2xyz(ra1, dec1, x1, y1, z1);
+    radec2xyz(ra2, dec2, x2, y2, z2);
+    return chord2(x1, y1, z1, x2, y2, z2);
+}
+
 // A source (a thread's object).
 struct AObj {
     double ra, dec;
-    double x, y, z;     // FP64 unit vector (computed on first use)
     float fx, fy, fz;
     double alpha;
     long long id;
     uint32_t gi;        // index in the A segment
     int zone;
     bool full_ring;     // alpha >= 3: every object of a zone is a candidate
-    bool have_xyz;
     Win w;              // quantised windows
 };
 
@@ -602,19 +557,6 @@ __device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, 
     return total;
 }
 
-// Zone of A object i of a tile spanning zones [zf, zl] (A zone offsets in
-// global memory); -1 if the offsets disagree (never for a consistent segment).
-__device__ __forceinline__ int a_zone(const uint32_t *__restrict__ a_zoff, int zf, int zl, uint32_t i)
-{
-    if (zf == zl) return zf;
-    int lo = zf, hi = zl;   // last z with a_zoff[z] <= i
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&a_zoff[mid]) <= i) lo = mid; else hi = mid - 1;
-    }
-    return (__ldg(&a_zoff[lo]) <= i && i < __ldg(&a_zoff[lo + 1])) ? lo : -1;
-}
-
 // Zone of A object i of the staged tile; -1 if the offsets disagree.
 template <class Stage>
 __device__ __forceinline__ int a_zone_s(const Stage &S, uint32_t i)
@@ -669,15 +611,7 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
                 if (cuts_pass(J, a, rb)) {
                     m = true;
                     if (band || DIST) {
-                        if (!a.have_xyz) {
-                            a.x = __ldg(&J.a_xyz64[3 * (size_t)a.gi]);
-                            a.y = __ldg(&J.a_xyz64[3 * (size_t)a.gi + 1]);
-                            a.z = __ldg(&J.a_xyz64[3 * (size_t)a.gi + 2]);
-                            a.have_xyz = true;
-                        }
-                        const size_t gb = 3 * (size_t)global_index(V, c.zb, q);
-                        c2 = chord2(a.x, a.y, a.z, __ldg(&J.b_xyz64[gb]), __ldg(&J.b_xyz64[gb + 1]),
-                                    __ldg(&J.b_xyz64[gb + 2]));
+                        c2 = chord2_radec(a.ra, a.dec, rb.x, rb.y);
                         if (band) {
                             cn.exact++;
                             m = c2 < J.sr_dist2;
@@ -1265,7 +1199,6 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 a.full_ring = a.alpha >= 3.0;
                 a.id = S.a_id[S.id_skew + t];
                 a.gi = S.a_start + t;
-                a.have_xyz = false;
                 BView V;
                 V.staged = false;
                 V.whole = false;
@@ -1319,8 +1252,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     a.full_ring = alpha >= 3.0;
                     a.id = S.a_id[S.id_skew + t];
                     a.gi = S.a_start + t;
-                    a.have_xyz = false;
-                    test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
+                        test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
                 }
             } else {
                 // inclusive scan of candidate counts across the warp
@@ -1383,24 +1315,24 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                             if (!(c32 > K.thr_hi)) {
                                 // below thr_lo the FP64 chord is under the threshold and, in a zone
                                 // with an RA cut (alpha < 3), the dec and RA cuts hold (bounds in
-                                // xm_make_params): B's ra/dec and the FP64 vectors are read only
-                                // inside the band, or for the distance
+                                // xm_make_params): B's ra/dec is read and the FP64 vectors are
+                                // computed only inside the band, or for the distance
                                 const bool band = c32 >= K.thr_lo;
                                 cn.border += band ? 1ull : 0ull;
                                 bool pass = true;
-                                if (band || al >= 3.0) {
+                                const bool cut = band || al >= 3.0;
+                                double2 rb = make_double2(0.0, 0.0);
+                                if (cut || DIST) {
                                     if (gq == 0xFFFFFFFFu) gq = staged_global(V, (int)S.nseg, q);
-                                    pass = cuts_k(K, ra.x, ra.y, al, __ldg(&J.b_radec[gq]));
+                                    rb = __ldg(&J.b_radec[gq]);
                                 }
+                                if (cut) pass = cuts_k(K, ra.x, ra.y, al, rb);
                                 if (pass) {
                                     m = true;
                                     if (band || DIST) {
-                                        if (gq == 0xFFFFFFFFu) gq = staged_global(V, (int)S.nseg, q);
-                                        const size_t ga = 3 * (size_t)(S.a_start + ta);
-                                        const size_t gb = 3 * (size_t)gq;
-                                        c2 = chord2(__ldg(&J.a_xyz64[ga]), __ldg(&J.a_xyz64[ga + 1]),
-                                                    __ldg(&J.a_xyz64[ga + 2]), __ldg(&J.b_xyz64[gb]),
-                                                    __ldg(&J.b_xyz64[gb + 1]), __ldg(&J.b_xyz64[gb + 2]));
+                                        // FP64 unit vectors of both ends, as the zone builder
+                                        // computes them (the same bits), then the chord
+                                        c2 = chord2_radec(ra.x, ra.y, rb.x, rb.y);
                                         if (band) {
                                             cn.exact++;
                                             m = c2 < K.sr_dist2;

@@ -11,11 +11,9 @@ struct JobDev {
     const double2 *a_radec;
     const float4 *a_xyz;
     const uint32_t *a_zoff;    // [n_zones + 1]
-    const double *a_xyz64;     // [3 nA] FP64 unit vectors
     const long long *b_id;
     const double2 *b_radec;
     const float4 *b_xyz;
-    const double *b_xyz64;
     const uint32_t *b_zoff;    // [n_zones + 1]
     const double *alpha;       // RA half-width of A's zone z at alpha[z - alpha_z0], z in [z_lo, z_hi]
     double sr_rad, sr_dist2;

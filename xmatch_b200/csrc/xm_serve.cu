@@ -81,12 +81,13 @@ struct xm_server {
 
 namespace {
 
-// Device bytes a query holds while in flight: its segment (64 B per object and
-// the zone offsets) and room for 2 n matches (16 B pairs, 8 B distance, 4 B
-// job index), the default output size of Worker.cu:296-297.
+// Device bytes a query holds while in flight: its segment (40 B per object:
+// id, ra/dec, FP32 unit vector; and the zone offsets) and room for 2 n matches
+// (16 B pairs, 8 B distance, 4 B job index), the default output size of
+// Worker.cu:296-297.
 uint64_t query_bytes(uint64_t n, int32_t n_zones)
 {
-    return 64 * n + 4 * ((uint64_t)n_zones + 8) + 28 * std::max<uint64_t>(2 * n, 1024);
+    return 40 * n + 4 * ((uint64_t)n_zones + 8) + 28 * std::max<uint64_t>(2 * n, 1024);
 }
 
 void builder_loop(xm_server *S)
@@ -221,6 +222,10 @@ extern "C" xm_status xm_serve_open(xm_ctx *ctx, const xm_segment *catalog, const
 {
     if (!ctx || !catalog || !out || catalog->ctx->device != ctx->device) return XM_ERR_INVALID;
     *out = nullptr;
+    if (!catalog->store) {
+        ctx->last_error = "the catalog segment is offloaded (xm_segment_page_in it first)";
+        return XM_ERR_INVALID;
+    }
     cudaSetDevice(ctx->device);
     auto *S = new xm_server();
     S->mctx = ctx;
