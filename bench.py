@@ -56,9 +56,9 @@ def parse():
                     help="keep only sources with dec in [LO, HI) deg (same density, smaller case for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
-    ap.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
+    ap.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4", "dense"],
                     help="c1: 50Mx50M crossmatch (the headline); c2: 4,096-job batch; c3: precision stress; "
-                         "c4: serving")
+                         "c4: serving; dense: FP32 filter against plain FP64 in dense clusters, by radius")
     ap.add_argument("--c2-jobs", type=int, default=4096)
     ap.add_argument("--c2-scale", type=float, default=1.0, help="scale of the c2 per-job sizes")
     ap.add_argument("--c3-n", type=int, default=10_000_000)
@@ -675,6 +675,52 @@ def run_c3(args):
     return 0
 
 
+def run_dense(args):
+    """Where the FP32 filter pays: the pair kernel with the FP32 chord filter against
+    the plain all-FP64 kernel (FP64 cuts, sincos per pair) as the candidates per
+    object grow -- catalogs of only the config-1 cluster component (500 Gaussian
+    clusters, sigma 0.1 deg; B = 70 % perturbed copies + 30 % random members), zone
+    height = radius, radii 1" .. 30"."""
+    import torch
+    import xmatch_b200 as xm
+    synth = _load_by_path("synth")
+    torch.cuda.set_device(0)
+    ctx = xm.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", 0))
+    rng = np.random.default_rng(1005)
+    n = 10_000_000
+    ra, dec, centers = synth.mixture(rng, n, frac_cluster=1.0)
+    A = synth.make_objs(np.arange(n), ra, dec)
+    npert = int(0.7 * n)
+    src = rng.integers(0, n, npert)
+    pra, pdec = synth.perturb(rng, ra[src], dec[src], 0.3 * ARCSEC)
+    rra, rdec, _ = synth.mixture(rng, n - npert, frac_cluster=1.0, centers=centers)
+    B = synth.make_objs(np.arange(n) + 100_000_000_000, np.concatenate([pra, rra]), np.concatenate([pdec, rdec]))
+    K, W = args.steps, max(args.warmup, 3)
+    rows = {}
+    for r_arcsec in (1.0, 3.0, 10.0, 30.0):
+        r = r_arcsec * ARCSEC
+        sa, sb = ctx.build(A, r), ctx.build(B, r)
+        _, _, st = ctx.match(sa, sb, r, xm.XM_COUNT_CAND, fetch=False)
+        t32 = event_ms(stream, lambda: ctx.match(sa, sb, r, xm.XM_NO_DIST, fetch=False), K, W)
+        t64 = event_ms(stream, lambda: ctx.match(sa, sb, r, xm.XM_PLAIN64 | xm.XM_NO_DIST, fetch=False), K, W)
+        k32 = ctx.match(sa, sb, r, xm.XM_NO_DIST, fetch=False)[2]["ms_match"]
+        k64 = ctx.match(sa, sb, r, xm.XM_PLAIN64 | xm.XM_NO_DIST, fetch=False)[2]["ms_match"]
+        rows["r=%g\"" % r_arcsec] = {
+            "candidates_per_object": st["n_cand"] / len(sa), "tested_per_object": st["n_tested"] / len(sa),
+            "matches": st["n_match"], "borderline_fraction": st["n_border"] / max(st["n_tested"], 1),
+            "ms_match_filter32": t32, "ms_match_plain64": t64, "pair_kernel_ms_filter32": k32,
+            "pair_kernel_ms_plain64": k64, "kernel_speedup_filter32_vs_plain64": k64 / k32}
+        sa.free()
+        sb.free()
+    emit(args, {"metric": "FP32 filter vs plain FP64 pair kernel, dense clusters", "unit": "ms",
+                "higher_is_better": False, "n_gpus": 1, "steps": K, "warmup": W, "dtype": "f64",
+                "data": "synthetic (500 Gaussian clusters of sigma 0.1 deg, seeded)",
+                "config": {"workload": "clusters only, %d x %d, zh = r" % (n, n)}, "results": rows})
+    ctx.close()
+    return 0
+
+
 def cap_points(rng, n, ra0, dec0, radius_deg):
     """n points uniform in the spherical cap of the given radius around (ra0, dec0)."""
     ct = rng.uniform(np.cos(np.radians(radius_deg)), 1.0, n)
@@ -786,6 +832,18 @@ def run_c4(args):
     lat = np.array([i["t_done_ms"] - i["t_submit_ms"] for i in infos])
     span_s = (max(i["t_done_ms"] for i in infos) - min(i["t_submit_ms"] for i in infos)) * 1e-3
     batches = np.array([i["batch_size"] for i in infos])
+    # where each query's latency goes: waiting for admission, its zone build, waiting
+    # for a batch, the batch's match (pair kernel + grouping), results to the host
+    parts = {"admit_wait": ("t_submit_ms", "t_admit_ms"), "build": ("t_admit_ms", "t_built_ms"),
+             "batch_wait": ("t_built_ms", "t_batch_ms"), "match": ("t_batch_ms", "t_matched_ms"),
+             "to_host": ("t_matched_ms", "t_done_ms")}
+    comp = {k: np.array([i[b] - i[a] for i in infos]) for k, (a, b) in parts.items()}
+    slow = np.argsort(lat)[-max(1, len(lat) // 100):]   # the slowest 1 %
+    breakdown = {k: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
+                     "mean_slowest_1pct": float(v[slow].mean())} for k, v in comp.items()}
+    slowest = [{"ms": float(lat[k]), "n": len(queries[k][0]), "r_arcsec": queries[k][1] * 3600,
+                "batch": int(infos[k]["batch"]), "batch_size": int(batches[k]),
+                **{p: float(comp[p][k]) for p in parts}} for k in slow[::-1]]
     # a sample alone: build + plain FP64 match + results to host, one query at a time
     alone64, alone32 = [], []
     for k in range(min(args.c4_alone, len(queries))):
@@ -808,6 +866,7 @@ def run_c4(args):
         "queries_per_s": len(queries) / span_s, "matches_per_s": matches / span_s, "matches": matches,
         "objects_per_s": sum(len(q) for q, _ in queries) / span_s,
         "batch_size": {"mean": float(batches.mean()), "max": int(batches.max())},
+        "latency_breakdown_ms": breakdown, "slowest_queries": slowest,
         "alone_first_%d_queries_ms" % m: {"plain64_mean": float(np.mean(alone64)),
                                           "filter32_mean": float(np.mean(alone32)),
                                           "served_latency_mean": float(np.mean(lat[:m]))},
@@ -828,6 +887,8 @@ def main():
         return run_c3(args)
     if args.config == "c4":
         return run_c4(args)
+    if args.config == "dense":
+        return run_dense(args)
     return run_ours(args)
 
 
