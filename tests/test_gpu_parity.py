@@ -368,7 +368,7 @@ def test_offloaded_segments_page_in_per_job(ctx, fixtures):
     zh = 5 * ARCSEC
     segs = [ctx.build(a[s:s + 2500], zh, k) for k, s in enumerate(range(0, len(a), 2500))]
     B = ctx.build(a2, zh, 9)
-    want = [sp(ctx.match(s, B, zh, xm.XM_NO_DIST)[0]) for s in segs]
+    want = [sp(ctx.match(s, B, zh, with_dist=False)[0]) for s in segs]
     ids0 = segs[0].export()
     for s in segs:
         s.offload()
@@ -381,7 +381,7 @@ def test_offloaded_segments_page_in_per_job(ctx, fixtures):
         for k, s in enumerate(segs):
             if k + 1 < len(segs):
                 segs[k + 1].page_in()
-            p = sp(ctx.match(s, B, zh, xm.XM_NO_DIST)[0])
+            p = sp(ctx.match(s, B, zh, with_dist=False)[0])
             assert np.array_equal(p, want[k]), (rep, k)
             s.page_out()
     for s in segs:

@@ -876,7 +876,10 @@ static xm_status copy_out(xm_ctx *ctx, const int64_t *dpairs, const double *ddis
     XM_CUDA(ctx, cudaEventRecord(ctx->ev[4], st));
     if (out->pairs && count) XM_CUDA(ctx, cudaMemcpyAsync(out->pairs, dpairs, count * 16, cudaMemcpyDeviceToHost, st));
     if (out->dist && count) {
-        if (!ctx->res.has_dist) return XM_ERR_INVALID;
+        if (!ctx->res.has_dist) {
+            ctx->last_error = "distances asked for, but the match ran with XM_NO_DIST";
+            return XM_ERR_INVALID;
+        }
         XM_CUDA(ctx, cudaMemcpyAsync(out->dist, ddist, count * 8, cudaMemcpyDeviceToHost, st));
     }
     XM_CUDA(ctx, cudaEventRecord(ctx->ev[5], st));

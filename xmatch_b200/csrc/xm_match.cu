@@ -125,10 +125,8 @@ __device__ __forceinline__ Win make_win(double ra, double alpha, int shift)
 }
 
 // FP64 chord^2 of two positions from their unit vectors, computed as the zone
-// builder computes them (the same bits).  Out of line: it runs for the few
-// pairs inside the FP32 margin band (and for distances), and keeping its
-// registers out of the pair loop keeps the loop's occupancy.
-__device__ __noinline__ double chord2_radec(double ra1, double dec1, double ra2, double dec2)
+// builder computes them (the same bits).
+__device__ __forceinline__ double chord2_radec(double ra1, double dec1, double ra2, double dec2)
 {
     double x1, y1, z1, x2, y2, z2;
     radec2xyz(ra1, dec1, x1, y1, z1);
