@@ -36,7 +36,7 @@ def sp(p, d=None):
 def gpu_pairs(ctx, A, B, r, zh, flags):
     import xmatch_b200 as xm
     sa, sb = ctx.build(A, zh, 0), ctx.build(B, zh, 1)
-    p, d, st = ctx.match(sa, sb, r, flags | xm.XM_COUNT_CAND)
+    p, d, st = ctx.match(sa, sb, r, flags | xm.XM_COUNT_CAND, with_dist=not (flags & xm.XM_NO_DIST))
     sa.free()
     sb.free()
     return p, d, st

@@ -323,6 +323,18 @@ struct ZRec {          // 32 bytes, one per kept object
 };
 constexpr uint32_t kRaqMask = (1u << kRaqBits) - 1u;
 
+// A ZRec moves in one 256-bit global access (sm_100's widest): one store
+// transaction per scattered record instead of two, which measured 1.73 against
+// 2.49 ms for the scatter of 50M records when half of each record was written.
+__device__ __forceinline__ void st_rec(ZRec *q, double ra, double dec, unsigned long long id, uint32_t key,
+                                       uint32_t idx)
+{
+    const unsigned long long w3 = ((unsigned long long)idx << 32) | key;
+    asm volatile("st.global.v4.b64 [%0], {%1, %2, %3, %4};" ::"l"(q), "l"(__double_as_longlong(ra)),
+                 "l"(__double_as_longlong(dec)), "l"(id), "l"(w3)
+                 : "memory");
+}
+
 // ---- record tiles streamed through shared memory (scatter pass) ----
 // A block walks its tiles of kTileRecs records through two shared-memory
 // buffers.  A full tile of a 16-byte aligned input is one bulk asynchronous
@@ -562,13 +574,8 @@ zc_scatter(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp, 
                 const uint32_t i = threadIdx.x + (uint32_t)u * kStageThreads;
                 const double ra = __ddiv_rn(rec_ra(w, i), XM_RAD2DEG);
                 const double dec = __ddiv_rn(rec_dec(w, i), XM_RAD2DEG);
-                const unsigned long long id = w[3 * i];
-                ZRec *q = recs + b0 + (lane - head[u]);
-                reinterpret_cast<double2 *>(q)[0] = make_double2(ra, dec);
-                reinterpret_cast<uint4 *>(q)[1] =
-                    make_uint4((uint32_t)id, (uint32_t)(id >> 32),
-                               (uint32_t)zl[u] << kRaqBits | xm::raq32(ra) >> (32 - kRaqBits),
-                               (uint32_t)(first + i));
+                st_rec(recs + b0 + (lane - head[u]), ra, dec, w[3 * i],
+                       (uint32_t)zl[u] << kRaqBits | xm::raq32(ra) >> (32 - kRaqBits), (uint32_t)(first + i));
             }
         }
     });
@@ -583,14 +590,14 @@ struct ZOut {
 
 __device__ __forceinline__ ZRec zs_load(const ZRec *p)
 {
-    const double2 a = reinterpret_cast<const double2 *>(p)[0];
-    const uint4 b = reinterpret_cast<const uint4 *>(p)[1];
+    unsigned long long a, b, c, d;
+    asm volatile("ld.global.v4.b64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p) : "memory");
     ZRec r;
-    r.ra = a.x;
-    r.dec = a.y;
-    r.id = (long long)(((unsigned long long)b.y << 32) | b.x);
-    r.raq = b.z;
-    r.idx = b.w;
+    r.ra = __longlong_as_double((long long)a);
+    r.dec = __longlong_as_double((long long)b);
+    r.id = (long long)c;
+    r.raq = (uint32_t)d;
+    r.idx = (uint32_t)(d >> 32);
     return r;
 }
 
@@ -657,15 +664,21 @@ __device__ __forceinline__ void zs_rank_zone(uint32_t m, K key_of, WarpSort &W, 
         if (k < m) W.key[W.base[sub[e]] + slot[e]] = key[e];
     }
     __syncwarp();
+    // rank = entries of the group with a smaller key, an equal key counting by its
+    // slot (keys are distinct here -- the input index is part of them -- but the
+    // ranks stay a permutation whatever the keys)
     uint32_t rank[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const uint32_t k = lane + 32u * e;
         rank[e] = 0;
         if (k < m) {
-            const uint32_t b0 = W.base[sub[e]], b1 = b0 + W.cnt[sub[e]];
+            const uint32_t b0 = W.base[sub[e]], b1 = b0 + W.cnt[sub[e]], me = b0 + slot[e];
             uint32_t r = b0;
-            for (uint32_t q = b0; q < b1; ++q) r += W.key[q] < key[e] ? 1u : 0u;
+            for (uint32_t q = b0; q < b1; ++q) {
+                const unsigned long long kq = W.key[q];
+                r += (kq < key[e] || (kq == key[e] && q < me)) ? 1u : 0u;
+            }
             rank[e] = r;
         }
     }

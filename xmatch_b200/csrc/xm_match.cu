@@ -126,12 +126,27 @@ __device__ __forceinline__ Win make_win(double ra, double alpha, int shift)
 
 // FP64 chord^2 of two positions from their unit vectors, computed as the zone
 // builder computes them (the same bits).
-__device__ __forceinline__ double chord2_radec(double ra1, double dec1, double ra2, double dec2)
+__device__ __forceinline__ double chord2_radec_inl(double ra1, double dec1, double ra2, double dec2)
 {
     double x1, y1, z1, x2, y2, z2;
     radec2xyz(ra1, dec1, x1, y1, z1);
     radec2xyz(ra2, dec2, x2, y2, z2);
     return chord2(x1, y1, z1, x2, y2, z2);
+}
+
+// Without distances the chord is needed only for the few pairs inside the FP32
+// margin band: out of line, which measured faster than inlined (3.75 against
+// 4.05 ms at 50M x 50M).  With distances it runs for every match: inlined
+// (4.95 against 6.19 ms).
+__device__ __noinline__ double chord2_radec_call(double ra1, double dec1, double ra2, double dec2)
+{
+    return chord2_radec_inl(ra1, dec1, ra2, dec2);
+}
+
+template <bool DIST>
+__device__ __forceinline__ double chord2_radec(double ra1, double dec1, double ra2, double dec2)
+{
+    return DIST ? chord2_radec_inl(ra1, dec1, ra2, dec2) : chord2_radec_call(ra1, dec1, ra2, dec2);
 }
 
 // A source (a thread's object).
@@ -609,7 +624,7 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
                 if (cuts_pass(J, a, rb)) {
                     m = true;
                     if (band || DIST) {
-                        c2 = chord2_radec(a.ra, a.dec, rb.x, rb.y);
+                        c2 = chord2_radec<DIST>(a.ra, a.dec, rb.x, rb.y);
                         if (band) {
                             cn.exact++;
                             m = c2 < J.sr_dist2;
@@ -1330,7 +1345,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                                     if (band || DIST) {
                                         // FP64 unit vectors of both ends, as the zone builder
                                         // computes them (the same bits), then the chord
-                                        c2 = chord2_radec(ra.x, ra.y, rb.x, rb.y);
+                                        c2 = chord2_radec<DIST>(ra.x, ra.y, rb.x, rb.y);
                                         if (band) {
                                             cn.exact++;
                                             m = c2 < K.sr_dist2;
