@@ -387,3 +387,20 @@ def test_offloaded_segments_page_in_per_job(ctx, fixtures):
     for s in segs:
         s.free()
     B.free()
+
+
+@pytest.mark.parametrize("zh_arcsec", [15, 30, 60])
+def test_bin_index_dense_zones(ctx, zh_arcsec):
+    """Segments dense enough for the per-zone bin index (8, 16 and 32 bins per zone at
+    these zone heights): the window search that starts inside the bin of the window's
+    lower end gives the oracle's pairs, wraparound and polar zones included."""
+    from xmatch_b200 import synth
+    rng = np.random.default_rng(16)
+    n = 800_000
+    ra, dec = synth.uniform_sphere(rng, n)
+    A = objs(np.arange(n), ra, dec)
+    k = n // 2
+    pra, pdec = synth.perturb(rng, ra[:k], dec[:k], 10 * ARCSEC)
+    rra, rdec = synth.uniform_sphere(rng, n - k)
+    B = objs(np.arange(n) + 10 ** 9, np.concatenate([pra, rra]), np.concatenate([pdec, rdec]))
+    check_parity(ctx, A, B, zh_arcsec)

@@ -656,6 +656,8 @@ xm_status prepare_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_
         d.b_id = (const long long *)B->id;
         d.b_radec = B->radec;
         d.b_xyz = B->xyz;
+        d.b_bins = B->zbin;
+        d.b_bin_log2 = B->zbin ? B->bin_log2 : 0;
         d.b_zoff = B->zone_off;
         d.sr_rad = p.sr_rad;
         d.sr_dist2 = p.sr_dist2;

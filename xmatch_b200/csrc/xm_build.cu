@@ -586,7 +586,49 @@ struct ZOut {
     long long *id;
     double2 *radec;
     float4 *xyz;
+    uint16_t *zbin;    // per-zone bin index, or null
+    int bin_log2;
 };
+
+// Per-zone bin index of a segment (xm_segment::zbin).  With K = 2^bin_log2
+// bins of the quantised-ra turn, entry j of zone z's row is the number of the
+// zone's objects whose raq is below (j + 1) << (kRaqBits - bin_log2), i.e.
+// the start of bin j + 1 relative to the zone's first object (saturated at
+// 0xFFFF).  The pair kernel's window search starts inside the bin of the
+// window's lower end instead of bisecting the whole zone.  One warp per zone:
+// a shared-memory histogram of the zone's bins, then its inclusive scan.
+template <class R>
+__device__ __forceinline__ void zone_bins_warp(uint32_t mz, R raq_of, uint32_t *hist, uint16_t *row, int bin_log2,
+                                               unsigned lane)
+{
+    hist[lane] = 0;
+    __syncwarp();
+    for (uint32_t q = lane; q < mz; q += 32) atomicAdd(&hist[raq_of(q) >> (kRaqBits - bin_log2)], 1u);
+    __syncwarp();
+    uint32_t incl = hist[lane];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= (unsigned)d) incl += y;
+    }
+    if ((int)lane < (1 << bin_log2)) row[lane] = (uint16_t)min(incl, 0xFFFFu);
+    __syncwarp();
+}
+
+// The index of a sorted segment from its quantised ra (xyz.w), one warp per
+// zone (the radix-sort build).
+__global__ void zb_bins(const float4 *__restrict__ xyz, const uint32_t *__restrict__ zone_off, int n_zones,
+                        int bin_log2, uint16_t *__restrict__ zbin)
+{
+    __shared__ uint32_t hist[8][32];
+    const unsigned lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    for (int z = blockIdx.x * 8 + w; z < n_zones; z += gridDim.x * 8) {
+        const uint32_t b = zone_off[z], m = zone_off[z + 1] - b;
+        zone_bins_warp(m, [&](uint32_t q) { return __float_as_uint(xyz[b + q].w) & kRaqMask; }, hist[w],
+                       zbin + ((size_t)z << bin_log2), bin_log2, lane);
+    }
+}
 
 __device__ __forceinline__ ZRec zs_load(const ZRec *p)
 {
@@ -623,6 +665,7 @@ struct WarpSort {
     unsigned long long key[kWarpZone];   // keys grouped by raq sub-range
     uint16_t at[kWarpZone];              // zone entry at each rank
     uint32_t cnt[32], base[32];
+    uint32_t hist[32];                   // bin index histogram
 };
 
 // Ranks the m <= kWarpZone keys key_of(0..m) of one zone by value (distinct:
@@ -790,13 +833,21 @@ zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint
         __syncthreads();
         for (int k = warp; k < nzb; k += kBucketWarps) {
             const uint32_t zb = S.zbeg[k], mz = S.zbeg[k + 1] - zb;
+            if (o.zbin) {   // the zone's bin index (the order inside the zone does not matter)
+                uint16_t *row = o.zbin + ((size_t)(z0 + k) << o.bin_log2);
+                if (in_smem)
+                    zone_bins_warp(mz, [&](uint32_t q) { return (uint32_t)(S.key[zb + q] >> 32); }, W.hist, row,
+                                   o.bin_log2, lane);
+                else
+                    zone_bins_warp(mz, [&](uint32_t q) { return (uint32_t)(zrec_key(recs_z + r0 + zb + q) >> 32); },
+                                   W.hist, row, o.bin_log2, lane);
+            }
             if (mz == 0) continue;
             if (mz > (uint32_t)kWarpZone) {   // zs_block sorts it from recs_z
                 if (in_smem)
                     for (uint32_t q = lane; q < mz; q += 32) {
-                        const ZRec *p = recs_b + r0 + S.pos[zb + q];
-                        reinterpret_cast<double2 *>(recs_z + r0 + zb + q)[0] = reinterpret_cast<const double2 *>(p)[0];
-                        reinterpret_cast<uint4 *>(recs_z + r0 + zb + q)[1] = reinterpret_cast<const uint4 *>(p)[1];
+                        const ZRec r = zs_load(recs_b + r0 + S.pos[zb + q]);
+                        st_rec(recs_z + r0 + zb + q, r.ra, r.dec, (unsigned long long)r.id, r.raq, r.idx);
                     }
                 continue;
             }
@@ -1002,6 +1053,11 @@ static xm_status build_lsd(xm_segment *seg, const xm_obj *objs, uint64_t n, xm_s
     zb_bounds_fill<<<grid_for((uint64_t)nz + 1, 256, ctx->sm_count, 8), 256, 0, st>>>(kin, n, raq_bits, nz,
                                                                                        seg->zone_off);
     launches++;
+    if (seg->zbin) {
+        zb_bins<<<grid_for((uint64_t)nz, 256, ctx->sm_count, 8), 256, 0, st>>>(seg->xyz, seg->zone_off, nz,
+                                                                                seg->bin_log2, seg->zbin);
+        launches++;
+    }
     XM_CUDA(ctx, cudaGetLastError());
     // dropped count beside the offsets
     seg->dropped_host = (uint32_t)dropped;
@@ -1034,6 +1090,19 @@ void xm_seg_layout(xm_segment *seg, void *base)
     seg->id = base ? (int64_t *)(w + seg->off_id) : nullptr;
     seg->radec = base ? (double2 *)(w + seg->off_radec) : nullptr;
     seg->xyz = base ? (float4 *)(w + seg->off_xyz) : nullptr;
+    seg->zbin = base && seg->bin_log2 ? (uint16_t *)(w + seg->off_zbin) : nullptr;
+}
+
+// Bins per zone of a segment's index: none below 16 objects per zone on
+// average (a bisection of a few steps is as fast), else about one bin per 2
+// to 4 objects, at most 32.
+static int bin_log2_for(uint64_t n, int32_t n_zones)
+{
+    const double avg = (double)n / std::max<int32_t>(n_zones, 1);
+    if (avg < 16) return 0;
+    if (avg < 32) return 3;
+    if (avg < 64) return 4;
+    return 5;
 }
 
 xm_status xm_seg_storage(xm_segment *seg, uint64_t n)
@@ -1046,15 +1115,18 @@ xm_status xm_seg_storage(xm_segment *seg, uint64_t n)
     if (seg->store && seg->cap >= n) return XM_OK;
     const uint64_t c = std::max<uint64_t>(n, 1);
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t bz = al(((size_t)seg->n_zones + 8) * 4), bi = al((c + 2) * 8), br = al(c * 16), bx = al(c * 16);
+    seg->bin_log2 = bin_log2_for(c, seg->n_zones);
+    const size_t bz = al(((size_t)seg->n_zones + 8) * 4), bi = al((c + 2) * 8), br = al(c * 16), bx = al(c * 16),
+                 bb = seg->bin_log2 ? al(((size_t)seg->n_zones << seg->bin_log2) * 2) : 0;
     xm_dev_free(ctx, seg->store);
     seg->store = nullptr;
     seg->cap = 0;
-    XM_TRY(xm_dev_alloc(ctx, &seg->store, bz + bi + br + bx));
-    seg->store_bytes = bz + bi + br + bx;
+    XM_TRY(xm_dev_alloc(ctx, &seg->store, bz + bi + br + bx + bb));
+    seg->store_bytes = bz + bi + br + bx + bb;
     seg->off_id = bz;
     seg->off_radec = bz + bi;
     seg->off_xyz = bz + bi + br;
+    seg->off_zbin = bz + bi + br + bx;
     xm_seg_layout(seg, seg->store);
     seg->cap = c;
     XM_CUDA(ctx, cudaMemsetAsync(seg->zone_off, 0, bz, ctx->stream));
@@ -1139,7 +1211,7 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
                  st>>>(objs, n, kp, shift, bulk_ok, bcur, recs_b, misc);
     launches++;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[10], st));
-    ZOut o{(long long *)seg->id, seg->radec, seg->xyz};
+    ZOut o{(long long *)seg->id, seg->radec, seg->xyz, seg->zbin, seg->bin_log2};
     zs_bucket<<<std::min(n_buckets, ctx->sm_count * 2), kBucketThreads, smem_bucket, st>>>(
         recs_b, recs_z, bcur, seg->zone_off, nz, shift, n_buckets, o, big, misc);
     zs_block<<<ctx->sm_count * 2, kZsThreads, smem_block, st>>>(recs_z, seg->zone_off, big, misc, o);

@@ -97,7 +97,8 @@ struct xm_segment {
     uint32_t dropped_host = 0;
     void *store = nullptr;         // one device allocation holding the arrays below (null when offloaded)
     size_t store_bytes = 0;        // its size, and the offsets of id, radec, xyz in it
-    size_t off_id = 0, off_radec = 0, off_xyz = 0;
+    size_t off_id = 0, off_radec = 0, off_xyz = 0, off_zbin = 0;
+    int bin_log2 = 0;              // 2^bin_log2 quantised-ra bins per zone in zbin (0 = no index)
     void *host_store = nullptr;    // pinned host copy of the store (xm_segment_offload)
     cudaEvent_t ready = nullptr;   // recorded after a page-in copy (xm_segment_page_in)
     bool ready_pending = false;    // work on ctx->stream must wait for `ready` first
@@ -106,6 +107,7 @@ struct xm_segment {
     int64_t *id = nullptr;
     double2 *radec = nullptr;      // radians
     float4 *xyz = nullptr;         // FP32 unit vector; w = quantised-ra bits
+    uint16_t *zbin = nullptr;      // [n_zones << bin_log2] per-zone bin index (see xm_build.cu)
 };
 // Points the segment's arrays into a store of its layout at base (null clears them).
 void xm_seg_layout(xm_segment *seg, void *base);

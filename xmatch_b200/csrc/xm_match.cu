@@ -174,7 +174,11 @@ struct BView {
     const uint32_t *off;
     const uint32_t *g;
     const uint32_t *zoff;
+    const uint16_t *bins;   // WHOLE: bin index rows of the band's zones (bin_log2 > 0)
+    int bin_log2;
 };
+
+constexpr int kRaqBitsB = 27;   // quantised-ra bits of the segments (xyz.w)
 
 // Candidate enumeration state: B zones of the band, and in each zone up to
 // three ra windows (direct, branch 2 with B near 0, branch 3 with B near 2 pi).
@@ -472,6 +476,20 @@ __device__ __forceinline__ int lane_ranges3(const BView &V, const Win &w, int zl
         if (zlo + k <= zhi) zone_range(V, zlo + k, b0[k], b1[k]);
         lo[k] = b0[k];
         hi[k] = b1[k];
+        if (V.bin_log2 && zlo + k <= zhi) {
+            // the zone's bin index: the first object with raq >= w.lo lies between the
+            // start of w.lo's bin and the start of the next bin (positions in the segment,
+            // then clipped to the staged piece as zone_range clips the zone)
+            const int kk = zlo + k - V.band_lo;
+            const uint32_t zs = V.zoff[kk], ze = V.zoff[kk + 1];
+            if (ze - zs < 0xFFFFu) {
+                const uint32_t bin = w.lo >> (kRaqBitsB - V.bin_log2);
+                const uint16_t *row = V.bins + (kk << V.bin_log2);
+                const uint32_t s0 = zs + (bin ? (uint32_t)row[bin - 1] : 0u), s1 = zs + (uint32_t)row[bin];
+                lo[k] = min(max(s0, V.base), V.base + V.len) - V.base;
+                hi[k] = min(max(s1, V.base), V.base + V.len) - V.base;
+            }
+        }
     }
     // first k in [b0, b1) with raq >= w.lo, per zone
     while (lo[0] < hi[0] || lo[1] < hi[1] || lo[2] < hi[2]) {
@@ -936,6 +954,8 @@ tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32
 // B's ra/dec are staged only for the all-FP64 variant (RADEC), which cuts every
 // candidate; the FP32 filter reads them from global memory for the few pairs
 // inside its margin band.  Without them a stage is small enough for three.
+constexpr int kBinZones = 4;   // band zones whose bin index rows a stage carries
+
 template <int TILE, bool RADEC>
 struct StageT {
     static constexpr int kCapB = 4 * TILE;
@@ -957,6 +977,9 @@ struct StageT {
     uint32_t alpha_skew, azo_skew;
     alignas(16) double alpha_s[kZcMax + 2];     // bulk-copy destinations: 16-byte aligned
     alignas(16) uint32_t azo_s[kZcMax + 8];
+    // B's bin index rows of the band (WHOLE plans of at most kBinZones zones)
+    alignas(16) uint16_t bins[kBinZones << 5];
+    uint32_t bin_log2;
 };
 
 template <int TILE, bool RADEC>
@@ -964,7 +987,7 @@ constexpr bool stage_aligned()
 {
     using S = StageT<TILE, RADEC>;
     return offsetof(S, zoff) % 16 == 0 && offsetof(S, a_id) % 16 == 0 && offsetof(S, a_radec) % 16 == 0 &&
-           offsetof(S, a_xyz) % 16 == 0 && offsetof(S, b_xyz) % 16 == 0;
+           offsetof(S, a_xyz) % 16 == 0 && offsetof(S, b_xyz) % 16 == 0 && offsetof(S, bins) % 16 == 0;
 }
 static_assert(stage_aligned<64, false>() && stage_aligned<128, false>() && stage_aligned<256, false>() &&
                   stage_aligned<64, true>() && stage_aligned<128, true>() && stage_aligned<256, true>(),
@@ -1013,10 +1036,11 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
         int cached_job = -1;
         const double2 *a_radec = nullptr, *b_radec = nullptr;
         const float4 *a_xyz = nullptr, *b_xyz = nullptr;
-        const long long *a_id = nullptr;
+        const long long *a_id = nullptr, *b_id = nullptr;
         const uint32_t *b_zoff = nullptr, *a_zoff = nullptr;
         const double *alpha = nullptr;
-        int alpha_z0 = 0;
+        const uint16_t *b_bins = nullptr;
+        int alpha_z0 = 0, b_bin_log2 = 0;
         // issue plan words w[16] into the next stage
         auto issue = [&](const uint32_t (&w)[16]) -> bool {
             if (!mbar_wait(&empty[s], phase ^ 1u)) return false;
@@ -1030,8 +1054,9 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 if ((int)job != cached_job) {
                     const JobDev &J = jobs[job];
                     a_radec = J.a_radec; a_xyz = J.a_xyz; a_id = J.a_id;
-                    b_radec = J.b_radec; b_xyz = J.b_xyz; b_zoff = J.b_zoff;
+                    b_radec = J.b_radec; b_xyz = J.b_xyz; b_zoff = J.b_zoff; b_id = J.b_id;
                     a_zoff = J.a_zoff; alpha = J.alpha; alpha_z0 = J.alpha_z0;
+                    b_bins = J.b_bins; b_bin_log2 = J.b_bin_log2;
                     cached_job = (int)job;
                 }
                 Stage &S = stages[s];
@@ -1061,6 +1086,9 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 bytes += acnt * 8u + azcnt * 4u;
                 uint32_t zcopy = 0, z_al = 0;
                 constexpr uint32_t kBBytes = RADEC ? 32u : 16u;   // staged bytes per B object
+                const bool bins = mode == PLAN_WHOLE && nseg <= (uint32_t)kBinZones && b_bin_log2 > 0;
+                S.bin_log2 = bins ? (uint32_t)b_bin_log2 : 0u;
+                if (bins) bytes += nseg << (b_bin_log2 + 1);
                 if (mode == PLAN_WHOLE) {
                     bytes += b_len * kBBytes;
                     z_al = (uint32_t)band_lo & ~3u;
@@ -1089,10 +1117,17 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 bulk_g2s(S.azo_s, a_zoff + az_al, azcnt * 4u, &full[s]);
                 if (mode == PLAN_WHOLE) {
                     if (b_len) {
+                        // the band's B ids into L2: matches read them when a warp's buffer is
+                        // flushed (16-byte aligned, whole 16-byte units; ids carry 2 spare entries)
+                        const uint32_t i0 = b_start & ~1u, i1 = (b_start + b_len + 1) & ~1u;
+                        bulk_prefetch_l2(b_id + i0, (i1 - i0) * 8u);
                         if (RADEC) bulk_g2s(S.b_radec, b_radec + b_start, b_len * 16u, &full[s]);
                         bulk_g2s(S.b_xyz, b_xyz + b_start, b_len * 16u, &full[s]);
                     }
                     bulk_g2s(S.zoff, b_zoff + z_al, zcopy * 4u, &full[s]);
+                    if (bins)   // rows of 2^bin_log2 16-bit entries: 16-byte multiples
+                        bulk_g2s(S.bins, b_bins + ((size_t)band_lo << b_bin_log2), nseg << (b_bin_log2 + 1),
+                                 &full[s]);
                 } else if (mode == PLAN_UNION) {
 #pragma unroll
                     for (uint32_t q = 0; q < (uint32_t)kMaxPlanSeg; ++q) {
@@ -1218,6 +1253,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 V.xyz = J.b_xyz;
                 V.zoff = J.b_zoff;
                 V.band_lo = 0;
+                V.bins = nullptr;
+                V.bin_log2 = 0;
                 test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
             }
         } else {
@@ -1231,6 +1268,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             V.len = S.b_len;
             V.off = S.seg_off;
             V.g = S.seg_g;
+            V.bins = S.bins;
+            V.bin_log2 = (int)S.bin_log2;
             // ---- phase 1: each lane's candidate ranges ----
             WList &L = wl[warp - 1];
             int n = 0, nr = 0, za = 0;

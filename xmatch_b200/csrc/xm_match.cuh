@@ -14,6 +14,8 @@ struct JobDev {
     const long long *b_id;
     const double2 *b_radec;
     const float4 *b_xyz;
+    const uint16_t *b_bins;    // B's per-zone bin index, or null (xm_segment::zbin)
+    int b_bin_log2;
     const uint32_t *b_zoff;    // [n_zones + 1]
     const double *alpha;       // RA half-width of A's zone z at alpha[z - alpha_z0], z in [z_lo, z_hi]
     double sr_rad, sr_dist2;
