@@ -630,16 +630,32 @@ __global__ void zb_bins(const float4 *__restrict__ xyz, const uint32_t *__restri
     }
 }
 
-__device__ __forceinline__ ZRec zs_load(const ZRec *p)
+// A record of a buffer the running kernel does not write: one 256-bit load
+// through the read-only path.
+__device__ __forceinline__ ZRec zs_load_ro(const ZRec *p)
 {
     unsigned long long a, b, c, d;
-    asm volatile("ld.global.v4.b64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p) : "memory");
+    asm("ld.global.nc.v4.b64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
     ZRec r;
     r.ra = __longlong_as_double((long long)a);
     r.dec = __longlong_as_double((long long)b);
     r.id = (long long)c;
     r.raq = (uint32_t)d;
     r.idx = (uint32_t)(d >> 32);
+    return r;
+}
+
+// A record the running kernel's block wrote (before a barrier): coherent loads.
+__device__ __forceinline__ ZRec zs_load(const ZRec *p)
+{
+    const double2 a = reinterpret_cast<const double2 *>(p)[0];
+    const uint4 b = reinterpret_cast<const uint4 *>(p)[1];
+    ZRec r;
+    r.ra = a.x;
+    r.dec = a.y;
+    r.id = (long long)(((unsigned long long)b.y << 32) | b.x);
+    r.raq = b.z;
+    r.idx = b.w;
     return r;
 }
 
@@ -846,7 +862,7 @@ zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint
             if (mz > (uint32_t)kWarpZone) {   // zs_block sorts it from recs_z
                 if (in_smem)
                     for (uint32_t q = lane; q < mz; q += 32) {
-                        const ZRec r = zs_load(recs_b + r0 + S.pos[zb + q]);
+                        const ZRec r = zs_load_ro(recs_b + r0 + S.pos[zb + q]);
                         st_rec(recs_z + r0 + zb + q, r.ra, r.dec, (unsigned long long)r.id, r.raq, r.idx);
                     }
                 continue;
@@ -854,7 +870,7 @@ zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint
             if (in_smem) {
                 zs_rank(mz, [&](uint32_t q) { return S.key[zb + q]; }, W, lane);
                 for (uint32_t p = lane; p < mz; p += 32)
-                    zs_emit(zs_load(recs_b + r0 + S.pos[zb + W.at[p]]), (unsigned long long)r0 + zb + p, o);
+                    zs_emit(zs_load_ro(recs_b + r0 + S.pos[zb + W.at[p]]), (unsigned long long)r0 + zb + p, o);
             } else {
                 const ZRec *zr = recs_z + r0 + zb;
                 zs_rank(mz, [&](uint32_t q) { return zrec_key(zr + q); }, W, lane);
@@ -913,7 +929,7 @@ zs_block(const ZRec *__restrict__ recs, const uint32_t *__restrict__ zone_off, c
         }
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < m; k += blockDim.x)
-            zs_emit(zs_load(recs + b + sp[k]), (unsigned long long)b + k, o);
+            zs_emit(zs_load_ro(recs + b + sp[k]), (unsigned long long)b + k, o);
         __syncthreads();
     }
 }

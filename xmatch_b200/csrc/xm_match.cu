@@ -954,7 +954,7 @@ tiles_make(const JobDev *__restrict__ jobs, int n_jobs, uint32_t n_items, uint32
 // B's ra/dec are staged only for the all-FP64 variant (RADEC), which cuts every
 // candidate; the FP32 filter reads them from global memory for the few pairs
 // inside its margin band.  Without them a stage is small enough for three.
-constexpr int kBinZones = 4;   // band zones whose bin index rows a stage carries
+constexpr int kBinZones = 8;   // band zones whose bin index rows a stage carries
 
 template <int TILE, bool RADEC>
 struct StageT {
