@@ -348,11 +348,11 @@ def run_ours(args):
         "zb_count": 24 * nc,                       # records in
         "zb_offsets": 16 * n_zones,                # counts in, offsets out, cursors
         "zb_scatter": (24 + 32) * nc,              # records in, 32-byte bucket records out
-        "zb_zone_sort": (32 + 64) * nc,            # bucket records in; id, radec, xyz, xyz64 out
+        "zb_zone_sort": (32 + 40) * nc,            # bucket records in; id, radec, xyz out
         "pair_plan": 64 * int(np.ceil(len(sa) / 128)),   # one 64-byte plan per tile
         # A once (id, radec, FP32 xyz), B's FP32 xyz once, per match B's id and the pair out; with
-        # distances also the distance and the FP64 vectors of both ends of every match
-        "pair_kernel": 40 * kept_a + 16 * kept_b + (24 + 8 + 48 if args.dist else 24) * n_match,
+        # distances also the distance out and B's ra/dec in (the FP64 vectors are recomputed)
+        "pair_kernel": 40 * kept_a + 16 * kept_b + (24 + 8 + 16 if args.dist else 24) * n_match,
     }
     peaks, peak_kind = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
@@ -361,14 +361,12 @@ def run_ours(args):
         gbs = alg_bytes[k] / (t * 1e-3) / 1e9 if t > 0 else 0.0
         stages[k] = {"ms": t, "alg_bytes": alg_bytes[k], "GB/s": gbs, "frac": gbs / hbm}
     dom = max(per, key=per.get)
-    # DRAM bytes (read + write) per launch from ncu captures of the same kernels on the config-1 catalogs
-    # cut to a dec band (same objects per zone), scaled by the objects a launch processes: the zone build
-    # and plan kernels on dec 0..10 deg, the pair kernel on dec 30..60 deg
-    band_a = 4_397_838
-    band_a_pair = 8_919_127
-    traffic_per_obj = {"pair_kernel": (586.95e6 + 90.34e6) / band_a_pair,
-                       "zb_scatter": (105.69e6 + 89.51e6) / band_a,
-                       "zb_zone_sort": (237.64e6 + 368.32e6) / band_a, "pair_plan": 3.01e6 / band_a}
+    # DRAM bytes (read + write) per launch from one-kernel ncu captures of the same kernels on the config-1
+    # catalogs cut to dec 30..60 deg (same objects per zone; 8,919,127 A objects), scaled by the objects a
+    # launch processes
+    band_a = 8_919_127
+    traffic_per_obj = {"pair_kernel": (583.38e6 + 91.16e6) / band_a, "zb_scatter": (214.17e6 + 235.99e6) / band_a,
+                       "zb_zone_sort": (287.04e6 + 311.99e6) / band_a, "pair_plan": 3.01e6 / 4_397_838}
     units = {"pair_kernel": kept_a, "pair_plan": kept_a, "zb_scatter": nc, "zb_zone_sort": nc}
     for k in stages:
         if k in traffic_per_obj:
@@ -378,7 +376,9 @@ def run_ours(args):
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per object on a dec-band cut of "
                                   "the same catalogs, times the objects of this launch",
                 "peak_source": peak_kind}
-    pipeline_bytes = (24 + 64) * (n + nb) + 40 * kept_a + 16 * kept_b + (32 if args.dist else 24) * n_match
+    # per catalog: records read (24) and the sorted SoA written (40); the pair kernel: A read once (40), B's
+    # FP32 vectors read once (16), per match the record out (16 or 24) and B's id (8)
+    pipeline_bytes = (24 + 40) * (n + nb) + 40 * kept_a + 16 * kept_b + (32 if args.dist else 24) * n_match
     pipeline = {"alg_bytes": pipeline_bytes, "GB/s": pipeline_bytes / (ms * 1e-3) / 1e9,
                 "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / hbm}
     value = whole_job_rate(world, n_cand, ms)

@@ -708,6 +708,22 @@ xm_status xm_run_jobs(xm_ctx *ctx, const xm_job *jobs, uint32_t n_jobs, uint32_t
     L.variant = (flags & XM_PLAIN64) ? 1 : 0;
     L.count_cand = (flags & XM_COUNT_CAND) != 0;
     L.dist = (flags & XM_NO_DIST) == 0;
+    // Default geometry.  Where A's populated zones hold 48 or more objects on average, a
+    // zone is split into tiles anyway, so the wider tile of 256 objects (8 consumer warps)
+    // packs two to three zones and keeps its lanes busy, with items of 32 zones: at 50M x 50M
+    // (77 objects per zone) 3.43 against 3.92 ms for tiles of 128.
+    {
+        uint64_t objs = 0, zones = 0;
+        for (uint32_t j = 0; j < n_jobs; ++j)
+            if (jobs[j].A && jobs[j].A->n > 0 && jobs[j].A->z_hi >= jobs[j].A->z_lo) {
+                objs += jobs[j].A->n;
+                zones += (uint64_t)(jobs[j].A->z_hi - jobs[j].A->z_lo + 1);
+            }
+        if (zones && objs >= 48 * zones) {
+            L.tile = 256;
+            L.zc = 32;
+        }
+    }
     if (tuning) {
         if (tuning->tile) L.tile = (int)tuning->tile;
         if (tuning->chunk) L.chunk = tuning->chunk;

@@ -770,6 +770,7 @@ __device__ __forceinline__ void zs_rank(uint32_t m, K key_of, WarpSort &W, unsig
 // A bucket of more than kBucketCap records orders its records through recs_z in
 // global memory instead of shared memory.
 constexpr int kBucketCap = 6144;
+constexpr uint16_t kNoRecord = 0xFFFF;   // a position of a zone sorted by zs_block
 constexpr int kBucketWarps = kBucketThreads / 32;
 
 struct BucketSmem {
@@ -864,13 +865,25 @@ zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint
                     for (uint32_t q = lane; q < mz; q += 32) {
                         const ZRec r = zs_load_ro(recs_b + r0 + S.pos[zb + q]);
                         st_rec(recs_z + r0 + zb + q, r.ra, r.dec, (unsigned long long)r.id, r.raq, r.idx);
+                        S.pos[zb + q] = kNoRecord;   // not written by the bucket's emit below
                     }
                 continue;
             }
             if (in_smem) {
+                // the zone's records in sorted order: pos[zb + p] = bucket position of rank p
                 zs_rank(mz, [&](uint32_t q) { return S.key[zb + q]; }, W, lane);
-                for (uint32_t p = lane; p < mz; p += 32)
-                    zs_emit(zs_load_ro(recs_b + r0 + S.pos[zb + W.at[p]]), (unsigned long long)r0 + zb + p, o);
+                uint16_t v[kWarpZone / 32];
+#pragma unroll
+                for (int e = 0; e < kWarpZone / 32; ++e) {
+                    const uint32_t p = lane + 32u * e;
+                    v[e] = p < mz ? S.pos[zb + W.at[p]] : (uint16_t)0;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int e = 0; e < kWarpZone / 32; ++e) {
+                    const uint32_t p = lane + 32u * e;
+                    if (p < mz) S.pos[zb + p] = v[e];
+                }
             } else {
                 const ZRec *zr = recs_z + r0 + zb;
                 zs_rank(mz, [&](uint32_t q) { return zrec_key(zr + q); }, W, lane);
@@ -880,6 +893,21 @@ zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint
             __syncwarp();
         }
         __syncthreads();
+        if (in_smem) {
+            // the whole block writes the bucket's SoA in order, two records per thread in
+            // flight: every lane busy whatever the zone sizes, writes contiguous across zones
+            const uint32_t mc = S.zbeg[32];   // records placed in the bucket's zones (= m)
+            for (uint32_t j = threadIdx.x; j < mc; j += 2 * blockDim.x) {
+                const uint32_t j2 = j + blockDim.x;
+                const uint16_t q1 = S.pos[j], q2 = j2 < mc ? S.pos[j2] : kNoRecord;
+                ZRec r1, r2;
+                if (q1 != kNoRecord) r1 = zs_load_ro(recs_b + r0 + q1);
+                if (q2 != kNoRecord) r2 = zs_load_ro(recs_b + r0 + q2);
+                if (q1 != kNoRecord) zs_emit(r1, (unsigned long long)r0 + j, o);
+                if (q2 != kNoRecord) zs_emit(r2, (unsigned long long)r0 + j2, o);
+            }
+            __syncthreads();
+        }
     }
 }
 
