@@ -844,6 +844,22 @@ def run_c4(args):
     slowest = [{"ms": float(lat[k]), "n": len(queries[k][0]), "r_arcsec": queries[k][1] * 3600,
                 "batch": int(infos[k]["batch"]), "batch_size": int(batches[k]),
                 **{p: float(comp[p][k]) for p in parts}} for k in slow[::-1]]
+    # the batches of the slowest queries: every member, and the match time of each member alone
+    slow_batches = {}
+    for k in slow:
+        b = int(infos[k]["batch"])
+        if b in slow_batches:
+            continue
+        members = [j for j in range(len(infos)) if int(infos[j]["batch"]) == b]
+        rows = []
+        for j in members:
+            q, r = queries[j]
+            s_ = ctx.build(q, zh)
+            st_ = ctx.match(s_, cat, r, 0, fetch=False)[2]
+            s_.free()
+            rows.append({"n": len(q), "r_arcsec": r * 3600, "match_alone_ms": st_["ms_match"],
+                         "plan_alone_ms": st_["ms_plan"], "matches": st_["n_match"]})
+        slow_batches[b] = rows
     # a sample alone: build + plain FP64 match + results to host, one query at a time
     alone64, alone32 = [], []
     for k in range(min(args.c4_alone, len(queries))):
@@ -866,7 +882,7 @@ def run_c4(args):
         "queries_per_s": len(queries) / span_s, "matches_per_s": matches / span_s, "matches": matches,
         "objects_per_s": sum(len(q) for q, _ in queries) / span_s,
         "batch_size": {"mean": float(batches.mean()), "max": int(batches.max())},
-        "latency_breakdown_ms": breakdown, "slowest_queries": slowest,
+        "latency_breakdown_ms": breakdown, "slowest_queries": slowest, "batches_of_slowest": slow_batches,
         "alone_first_%d_queries_ms" % m: {"plain64_mean": float(np.mean(alone64)),
                                           "filter32_mean": float(np.mean(alone32)),
                                           "served_latency_mean": float(np.mean(lat[:m]))},

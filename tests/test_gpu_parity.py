@@ -404,3 +404,20 @@ def test_bin_index_dense_zones(ctx, zh_arcsec):
     rra, rdec = synth.uniform_sphere(rng, n - k)
     B = objs(np.arange(n) + 10 ** 9, np.concatenate([pra, rra]), np.concatenate([pdec, rdec]))
     check_parity(ctx, A, B, zh_arcsec)
+
+
+@pytest.mark.parametrize("zh_arcsec,r_arcsec", [(15, 60), (10, 120)])
+def test_bin_index_radius_spanning_zones(ctx, zh_arcsec, r_arcsec):
+    """Radius of several zone heights over segments with a bin index: windows in 9 and
+    25 zones per object, searched in staged bands and (at 120") in global memory through
+    the segment's bin rows, against the oracle."""
+    from xmatch_b200 import synth
+    rng = np.random.default_rng(17)
+    n = 2_000_000
+    ra, dec = synth.uniform_sphere(rng, n)
+    A = objs(np.arange(n), ra, dec)
+    k = n // 2
+    pra, pdec = synth.perturb(rng, ra[:k], dec[:k], r_arcsec / 2 * ARCSEC)
+    rra, rdec = synth.uniform_sphere(rng, n - k)
+    B = objs(np.arange(n) + 10 ** 9, np.concatenate([pra, rra]), np.concatenate([pdec, rdec]))
+    check_parity(ctx, A, B, r_arcsec, zh_arcsec=zh_arcsec, variants=(0,))

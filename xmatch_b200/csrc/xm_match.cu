@@ -227,6 +227,28 @@ __device__ __forceinline__ uint32_t upper_gallop(const BView &V, uint32_t lo, ui
     return upper_v(V, lo, b, t);
 }
 
+// Narrows [lo, hi), the view positions of B zone zb, to the bin of raq t in the
+// zone's bin index (when the view carries one): the first object with raq >= t
+// lies between the start of t's bin and the start of the next bin.  Staged
+// WHOLE views index the band's rows and clip to the staged piece as zone_range
+// does; the global view indexes the segment's rows.
+__device__ __forceinline__ void bins_narrow(const BView &V, int zb, uint32_t t, uint32_t &lo, uint32_t &hi)
+{
+    if (!V.bin_log2 || (V.staged && !V.whole)) return;
+    const uint32_t kk = V.staged ? (uint32_t)(zb - V.band_lo) : (uint32_t)zb;
+    const uint32_t zs = V.zoff[kk], ze = V.zoff[kk + 1];
+    if (ze - zs >= 0xFFFFu) return;   // the index saturates: bisect the whole zone
+    const uint32_t bin = t >> (kRaqBitsB - V.bin_log2);
+    const uint16_t *row = V.bins + ((size_t)kk << V.bin_log2);
+    uint32_t s0 = zs + (bin ? (uint32_t)row[bin - 1] : 0u), s1 = zs + (uint32_t)row[bin];
+    if (V.staged) {
+        s0 = min(max(s0, V.base), V.base + V.len) - V.base;
+        s1 = min(max(s1, V.base), V.base + V.len) - V.base;
+    }
+    lo = s0;
+    hi = s1;
+}
+
 __device__ __forceinline__ void open_window(const BView &V, const AObj &a, Cursor &c)
 {
     c.j = c.j_end = 0;
@@ -238,7 +260,9 @@ __device__ __forceinline__ void open_window(const BView &V, const AObj &a, Curso
         return;
     }
     if (c.win == 0) {
-        c.j = lower_v(V, c.b0, c.b1, a.w.lo);
+        uint32_t lo = c.b0, hi = c.b1;
+        bins_narrow(V, c.zb, a.w.lo, lo, hi);
+        c.j = lower_v(V, lo, hi, a.w.lo);
         c.j_end = c.b1;
         c.hi_cur = a.w.hi;
         c.w1_lo = c.j;
@@ -476,20 +500,7 @@ __device__ __forceinline__ int lane_ranges3(const BView &V, const Win &w, int zl
         if (zlo + k <= zhi) zone_range(V, zlo + k, b0[k], b1[k]);
         lo[k] = b0[k];
         hi[k] = b1[k];
-        if (V.bin_log2 && zlo + k <= zhi) {
-            // the zone's bin index: the first object with raq >= w.lo lies between the
-            // start of w.lo's bin and the start of the next bin (positions in the segment,
-            // then clipped to the staged piece as zone_range clips the zone)
-            const int kk = zlo + k - V.band_lo;
-            const uint32_t zs = V.zoff[kk], ze = V.zoff[kk + 1];
-            if (ze - zs < 0xFFFFu) {
-                const uint32_t bin = w.lo >> (kRaqBitsB - V.bin_log2);
-                const uint16_t *row = V.bins + (kk << V.bin_log2);
-                const uint32_t s0 = zs + (bin ? (uint32_t)row[bin - 1] : 0u), s1 = zs + (uint32_t)row[bin];
-                lo[k] = min(max(s0, V.base), V.base + V.len) - V.base;
-                hi[k] = min(max(s1, V.base), V.base + V.len) - V.base;
-            }
-        }
+        if (zlo + k <= zhi) bins_narrow(V, zlo + k, w.lo, lo[k], hi[k]);
     }
     // first k in [b0, b1) with raq >= w.lo, per zone
     while (lo[0] < hi[0] || lo[1] < hi[1] || lo[2] < hi[2]) {
@@ -569,7 +580,9 @@ __device__ __forceinline__ int lane_ranges(const BView &V, const JobScalars &K, 
         if (full_ring) {
             XM_PUSH(b0, b1);
         } else {
-            const uint32_t j0 = lower_v(V, b0, b1, w.lo);
+            uint32_t s0 = b0, s1 = b1;
+            bins_narrow(V, zb, w.lo, s0, s1);
+            const uint32_t j0 = lower_v(V, s0, s1, w.lo);
             const uint32_t j1 = upper_gallop(V, j0, b1, w.hi);
             XM_PUSH(j0, j1);
             if (w.lo2 <= w.hi2 && w.hi2 >= raq_at(V.xyz, b0)) {
@@ -1253,8 +1266,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 V.xyz = J.b_xyz;
                 V.zoff = J.b_zoff;
                 V.band_lo = 0;
-                V.bins = nullptr;
-                V.bin_log2 = 0;
+                V.bins = J.b_bins;
+                V.bin_log2 = J.b_bin_log2;
                 test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
             }
         } else {
