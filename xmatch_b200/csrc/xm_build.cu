@@ -451,18 +451,6 @@ __device__ __forceinline__ Run warp_run(int v, unsigned lane)
     return r;
 }
 
-// The buckets' atomic cursors sit one per 32-byte sector (kCurStride words
-// apart): the scatter's returning atomics on neighbouring buckets then do not
-// share a sector at the L2.
-constexpr int kCurStride = 8;
-
-// Bucket offsets (the exclusive scan of the bucket counts) into the spread cursors.
-__global__ void zc_spread(const uint32_t *__restrict__ boff, int n_buckets, uint32_t *__restrict__ bcur)
-{
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n_buckets; b += gridDim.x * blockDim.x)
-        bcur[(size_t)b * kCurStride] = boff[b];
-}
-
 // Pass 1: objects per bucket of 2^shift zones (a shared-memory histogram when
 // the buckets fit, else run-aggregated global atomics), the populated zone
 // range (misc[0], misc[1]) and the dropped count (misc[2]).  Only ra and dec
@@ -577,7 +565,7 @@ zc_scatter(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp, 
             const Run r = warp_run(bk, lane);
             head[u] = r.head;
             base[u] = 0;
-            if (r.is_head && bk >= 0) base[u] = atomicAdd(&bcur[(size_t)bk * kCurStride], r.len);
+            if (r.is_head && bk >= 0) base[u] = atomicAdd(&bcur[bk], r.len);
         }
 #pragma unroll
         for (int u = 0; u < kPerThread; ++u) {
@@ -786,7 +774,9 @@ __device__ __forceinline__ void zs_rank(uint32_t m, K key_of, WarpSort &W, unsig
 {
     if (m <= 32) zs_rank_zone<1>(m, key_of, W, lane);
     else if (m <= 64) zs_rank_zone<2>(m, key_of, W, lane);
+    else if (m <= 96) zs_rank_zone<3>(m, key_of, W, lane);
     else if (m <= 128) zs_rank_zone<4>(m, key_of, W, lane);
+    else if (m <= 192) zs_rank_zone<6>(m, key_of, W, lane);
     else zs_rank_zone<8>(m, key_of, W, lane);
 }
 
@@ -826,7 +816,7 @@ zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint
     for (int bk = blockIdx.x; bk < n_buckets; bk += gridDim.x) {
         const int z0 = bk << shift;
         const int nzb = min(1 << shift, n_zones - z0);
-        const uint32_t r0 = bk ? bend[(size_t)(bk - 1) * kCurStride] : 0u, r1 = bend[(size_t)bk * kCurStride];
+        const uint32_t r0 = bk ? bend[bk - 1] : 0u, r1 = bend[bk];
         const uint32_t m = r1 - r0;
         if (threadIdx.x < 32) S.zcnt[threadIdx.x] = 0;
         __syncthreads();
@@ -1238,17 +1228,15 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     // counts and cursors, large-zone list, scan scratch, misc
     const size_t rb = (n * sizeof(ZRec) + 255) & ~(size_t)255;
     const size_t bb = (((size_t)n_buckets + 1) * 4 + 255) & ~(size_t)255;
-    const size_t bp = ((size_t)n_buckets * kCurStride * 4 + 255) & ~(size_t)255;
     const size_t zb = (((size_t)nz + 1) * 4 + 255) & ~(size_t)255;
     const size_t sb = (xm_scan_tmp_bytes((size_t)n_buckets) + 255) & ~(size_t)255;
     const size_t mb = 256;
-    XM_TRY(ensure(ctx, &ctx->build_tmp, &ctx->build_tmp_bytes, 2 * rb + 2 * bb + bp + zb + sb + mb));
+    XM_TRY(ensure(ctx, &ctx->build_tmp, &ctx->build_tmp_bytes, 2 * rb + 2 * bb + zb + sb + mb));
     char *w = (char *)ctx->build_tmp;
     ZRec *recs_b = (ZRec *)w; w += rb;
     ZRec *recs_z = (ZRec *)w; w += rb;
     uint32_t *bcnt = (uint32_t *)w; w += bb;
-    uint32_t *boff = (uint32_t *)w; w += bb;
-    uint32_t *bcur = (uint32_t *)w; w += bp;
+    uint32_t *bcur = (uint32_t *)w; w += bb;
     uint32_t *big = (uint32_t *)w; w += zb;
     void *scan_tmp = w; w += sb;
     uint32_t *misc = (uint32_t *)w;   // z_lo, z_hi, dropped, n_big, largest big zone, error bits
@@ -1279,9 +1267,8 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
                                                                                   bcnt, misc);
     launches++;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[8], st));
-    XM_CUDA(ctx, xm_scan_exclusive_u32(bcnt, boff, (size_t)n_buckets, scan_tmp, st));
-    zc_spread<<<grid_for((uint64_t)n_buckets, 256, ctx->sm_count, 4), 256, 0, st>>>(boff, n_buckets, bcur);
-    launches += 4;
+    XM_CUDA(ctx, xm_scan_exclusive_u32(bcnt, bcur, (size_t)n_buckets, scan_tmp, st));
+    launches += 3;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[9], st));
     const bool bulk_ok = ((uintptr_t)objs & 15) == 0;
     const uint64_t n_tiles = (n + kTileRecs - 1) / kTileRecs;
