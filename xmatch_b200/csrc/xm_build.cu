@@ -901,9 +901,7 @@ __device__ __forceinline__ void zs_rank(uint32_t m, K key_of, WarpSort &W, unsig
 {
     if (m <= 32) zs_rank_zone<1>(m, key_of, W, lane);
     else if (m <= 64) zs_rank_zone<2>(m, key_of, W, lane);
-    else if (m <= 96) zs_rank_zone<3>(m, key_of, W, lane);
     else if (m <= 128) zs_rank_zone<4>(m, key_of, W, lane);
-    else if (m <= 192) zs_rank_zone<6>(m, key_of, W, lane);
     else zs_rank_zone<8>(m, key_of, W, lane);
 }
 
