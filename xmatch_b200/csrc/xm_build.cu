@@ -582,133 +582,6 @@ zc_scatter(const xm_obj *__restrict__ objs, unsigned long long n, KeyParams kp, 
     if (!ok && threadIdx.x == 0) atomicOr(&misc[5], 2u);
 }
 
-constexpr bool kSlicedScatter = true;
-
-// ---- the scatter without global atomics (buckets that fit a shared-memory histogram) ----
-// The input is cut into G contiguous slices, one per block.  zc_count_rows stores each
-// block's bucket histogram as row j of a G x n_buckets table; zc_colscan turns every
-// bucket's column into the offsets of the slices inside the bucket (and the bucket
-// totals, scanned into bucket starts); zc_scatter_rows loads its row of cursors
-// into shared memory and places each record with a shared-memory atomic.  The same
-// records land in the same buckets as with zc_scatter, in another order inside a
-// bucket, which the bucket sort does not depend on.
-__global__ void __launch_bounds__(256)
-zc_count_rows(const xm_obj *__restrict__ objs, unsigned long long n, unsigned long long slice, KeyParams kp,
-              int shift, int n_buckets, uint32_t *__restrict__ rows, uint32_t *__restrict__ misc)
-{
-    extern __shared__ uint32_t s_hist[];   // [n_buckets]
-    __shared__ unsigned s_lo, s_hi, s_bad;
-    for (int i = threadIdx.x; i < n_buckets; i += blockDim.x) s_hist[i] = 0;
-    if (threadIdx.x == 0) {
-        s_lo = 0xFFFFFFFFu;
-        s_hi = 0u;
-        s_bad = 0u;
-    }
-    __syncthreads();
-    const unsigned lane = threadIdx.x & 31;
-    unsigned zlo = 0xFFFFFFFFu, zhi = 0u, bad = 0u;
-    const unsigned long long i0 = blockIdx.x * slice, i1 = min(n, i0 + slice);
-    for (unsigned long long wb = i0 + (threadIdx.x & ~31u) * kCountU; wb < i1; wb += blockDim.x * kCountU) {
-        double ra[kCountU], dec[kCountU];
-#pragma unroll
-        for (int u = 0; u < kCountU; ++u) {
-            const unsigned long long i = wb + 32u * u + lane;
-            ra[u] = 0.0;
-            dec[u] = 0.0;
-            if (i < i1) {
-                ra[u] = __ldg(&objs[i].ra_deg);
-                dec[u] = __ldg(&objs[i].dec_deg);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kCountU; ++u) {
-            const unsigned long long i = wb + 32u * u + lane;
-            if (i >= i1) continue;
-            const int z = rec_zone(ra[u], dec[u], kp);
-            if (z < 0) {
-                ++bad;
-            } else {
-                zlo = min(zlo, (unsigned)z);
-                zhi = max(zhi, (unsigned)z);
-                atomicAdd(&s_hist[z >> shift], 1u);
-            }
-        }
-    }
-    zlo = __reduce_min_sync(0xffffffffu, zlo);
-    zhi = __reduce_max_sync(0xffffffffu, zhi);
-    bad = __reduce_add_sync(0xffffffffu, bad);
-    if (lane == 0) {
-        atomicMin(&s_lo, zlo);
-        atomicMax(&s_hi, zhi);
-        atomicAdd(&s_bad, bad);
-    }
-    __syncthreads();
-    uint32_t *row = rows + (size_t)blockIdx.x * n_buckets;
-    for (int i = threadIdx.x; i < n_buckets; i += blockDim.x) row[i] = s_hist[i];
-    if (threadIdx.x == 0) {
-        if (s_lo != 0xFFFFFFFFu) atomicMin(&misc[0], s_lo);
-        atomicMax(&misc[1], s_hi);
-        if (s_bad) atomicAdd(&misc[2], s_bad);
-    }
-}
-
-// Column b of the G x n_buckets table: counts -> offsets of the slices inside the
-// bucket (exclusive), and the bucket's total.
-__global__ void zc_colscan(uint32_t *__restrict__ rows, int g, int n_buckets, uint32_t *__restrict__ tot)
-{
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n_buckets; b += gridDim.x * blockDim.x) {
-        uint32_t run = 0;
-        for (int j = 0; j < g; ++j) {
-            const size_t k = (size_t)j * n_buckets + b;
-            const uint32_t c = rows[k];
-            rows[k] = run;
-            run += c;
-        }
-        tot[b] = run;
-    }
-}
-
-__global__ void __launch_bounds__(256, 2)
-zc_scatter_rows(const xm_obj *__restrict__ objs, unsigned long long n, unsigned long long slice, KeyParams kp,
-                int shift, int n_buckets, const uint32_t *__restrict__ rows, const uint32_t *__restrict__ bstart,
-                ZRec *__restrict__ recs)
-{
-    extern __shared__ uint32_t s_cur[];   // [n_buckets]
-    const uint32_t *row = rows + (size_t)blockIdx.x * n_buckets;
-    for (int i = threadIdx.x; i < n_buckets; i += blockDim.x) s_cur[i] = bstart[i] + row[i];
-    __syncthreads();
-    const unsigned lane = threadIdx.x & 31;
-    const uint32_t zmask = (1u << shift) - 1u;
-    const unsigned long long i0 = blockIdx.x * slice, i1 = min(n, i0 + slice);
-    for (unsigned long long wb = i0 + (threadIdx.x & ~31u) * kCountU; wb < i1; wb += blockDim.x * kCountU) {
-        double ra[kCountU], dec[kCountU];
-        unsigned long long id[kCountU];
-#pragma unroll
-        for (int u = 0; u < kCountU; ++u) {
-            const unsigned long long i = wb + 32u * u + lane;
-            ra[u] = 0.0;
-            dec[u] = 0.0;
-            id[u] = 0;
-            if (i < i1) {
-                ra[u] = __ldg(&objs[i].ra_deg);
-                dec[u] = __ldg(&objs[i].dec_deg);
-                id[u] = (unsigned long long)__ldg(&objs[i].id);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kCountU; ++u) {
-            const unsigned long long i = wb + 32u * u + lane;
-            if (i >= i1) continue;
-            const int z = rec_zone(ra[u], dec[u], kp);
-            if (z < 0) continue;
-            const uint32_t slot = atomicAdd(&s_cur[z >> shift], 1u);
-            const double rr = __ddiv_rn(ra[u], XM_RAD2DEG), dd = __ddiv_rn(dec[u], XM_RAD2DEG);
-            st_rec(recs + slot, rr, dd, id[u], ((uint32_t)z & zmask) << kRaqBits | xm::raq32(rr) >> (32 - kRaqBits),
-                   (uint32_t)i);
-        }
-    }
-}
-
 struct ZOut {
     long long *id;
     double2 *radec;
@@ -1356,15 +1229,7 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     const size_t zb = (((size_t)nz + 1) * 4 + 255) & ~(size_t)255;
     const size_t sb = (xm_scan_tmp_bytes((size_t)n_buckets) + 255) & ~(size_t)255;
     const size_t mb = 256;
-    // buckets that fit a shared-memory histogram: the input in G contiguous slices, one per
-    // block, scattered without global atomics through a G x n_buckets table of slice offsets
-    const bool sliced = n_buckets <= kHistMax && kSlicedScatter;
-    const uint64_t n_groups = (n + 2047) / 2048;
-    const uint64_t g_want = std::min<uint64_t>((uint64_t)ctx->sm_count * 2, std::max<uint64_t>(n_groups, 1));
-    const uint64_t slice = ((n_groups + g_want - 1) / g_want) * 2048;
-    const int g_slices = (int)((n + slice - 1) / slice);
-    const size_t tb = sliced ? (((size_t)g_slices * n_buckets * 4 + 255) & ~(size_t)255) : 0;
-    XM_TRY(ensure(ctx, &ctx->build_tmp, &ctx->build_tmp_bytes, 2 * rb + 2 * bb + zb + sb + mb + tb));
+    XM_TRY(ensure(ctx, &ctx->build_tmp, &ctx->build_tmp_bytes, 2 * rb + 2 * bb + zb + sb + mb));
     char *w = (char *)ctx->build_tmp;
     ZRec *recs_b = (ZRec *)w; w += rb;
     ZRec *recs_z = (ZRec *)w; w += rb;
@@ -1372,8 +1237,7 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     uint32_t *bcur = (uint32_t *)w; w += bb;
     uint32_t *big = (uint32_t *)w; w += zb;
     void *scan_tmp = w; w += sb;
-    uint32_t *misc = (uint32_t *)w; w += mb;   // z_lo, z_hi, dropped, n_big, largest big zone, error bits
-    uint32_t *rows = sliced ? (uint32_t *)w : nullptr;
+    uint32_t *misc = (uint32_t *)w;   // z_lo, z_hi, dropped, n_big, largest big zone, error bits
     uint32_t launches = 0;
     static bool attr = false;
     const size_t smem_scatter = sizeof(TileRing), smem_bucket = sizeof(BucketSmem);
@@ -1381,8 +1245,6 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     if (!attr) {
         XM_CUDA(ctx, cudaFuncSetAttribute(zc_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kHistMax * 4));
-        XM_CUDA(ctx, cudaFuncSetAttribute(zc_count_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kHistMax * 4));
-        XM_CUDA(ctx, cudaFuncSetAttribute(zc_scatter_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kHistMax * 4));
         XM_CUDA(ctx, cudaFuncSetAttribute(zc_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_scatter));
         XM_CUDA(ctx, cudaFuncSetAttribute(zs_bucket, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bucket));
         XM_CUDA(ctx, cudaFuncSetAttribute(zs_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_block));
@@ -1395,9 +1257,7 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
     XM_CUDA(ctx, cudaMemsetAsync(misc, 0xFF, 4, st));
     KeyParams kp{seg->zh_deg, nz, 32 - raq_bits, raq_bits, passes};
     const uint64_t cgroups = (n + kCountU - 1) / kCountU;
-    if (sliced)
-        zc_count_rows<<<g_slices, 256, (size_t)n_buckets * 4, st>>>(objs, n, slice, kp, shift, n_buckets, rows, misc);
-    else if (n_buckets <= kHistMax)
+    if (n_buckets <= kHistMax)
         zc_count<true><<<grid_for(cgroups, 256, ctx->sm_count, 2), 256, (size_t)n_buckets * 4, st>>>(
             objs, n, kp, shift, n_buckets, bcnt, misc);
     else
@@ -1405,28 +1265,18 @@ static xm_status build_zones(xm_segment *seg, const xm_obj *objs, uint64_t n, xm
                                                                                   bcnt, misc);
     launches++;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[8], st));
-    if (sliced) {
-        zc_colscan<<<grid_for((uint64_t)n_buckets, 256, ctx->sm_count, 4), 256, 0, st>>>(rows, g_slices, n_buckets,
-                                                                                          bcnt);
-        launches++;
-    }
     XM_CUDA(ctx, xm_scan_exclusive_u32(bcnt, bcur, (size_t)n_buckets, scan_tmp, st));
     launches += 3;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[9], st));
-    if (sliced) {
-        zc_scatter_rows<<<g_slices, 256, (size_t)n_buckets * 4, st>>>(objs, n, slice, kp, shift, n_buckets, rows,
-                                                                       bcur, recs_b);
-    } else {
-        const bool bulk_ok = ((uintptr_t)objs & 15) == 0;
-        const uint64_t n_tiles = (n + kTileRecs - 1) / kTileRecs;
-        zc_scatter<<<(unsigned)std::min<uint64_t>(n_tiles, (uint64_t)ctx->sm_count * 2), kStageThreads,
-                     smem_scatter, st>>>(objs, n, kp, shift, bulk_ok, bcur, recs_b, misc);
-    }
+    const bool bulk_ok = ((uintptr_t)objs & 15) == 0;
+    const uint64_t n_tiles = (n + kTileRecs - 1) / kTileRecs;
+    zc_scatter<<<(unsigned)std::min<uint64_t>(n_tiles, (uint64_t)ctx->sm_count * 2), kStageThreads, smem_scatter,
+                 st>>>(objs, n, kp, shift, bulk_ok, bcur, recs_b, misc);
     launches++;
     if (stats) XM_CUDA(ctx, cudaEventRecord(ctx->ev[10], st));
     ZOut o{(long long *)seg->id, seg->radec, seg->xyz, seg->zbin, seg->bin_log2};
     zs_bucket<<<std::min(n_buckets, ctx->sm_count * 2), kBucketThreads, smem_bucket, st>>>(
-        recs_b, recs_z, sliced ? bcur + 1 : bcur, seg->zone_off, nz, shift, n_buckets, o, big, misc);
+        recs_b, recs_z, bcur, seg->zone_off, nz, shift, n_buckets, o, big, misc);
     zs_block<<<ctx->sm_count * 2, kZsThreads, smem_block, st>>>(recs_z, seg->zone_off, big, misc, o);
     launches += 2;
     XM_CUDA(ctx, cudaGetLastError());
