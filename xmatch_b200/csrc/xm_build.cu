@@ -778,28 +778,248 @@ __device__ __forceinline__ void zs_rank(uint32_t m, K key_of, WarpSort &W, unsig
     else zs_rank_zone<8>(m, key_of, W, lane);
 }
 
-// Pass 3, one block per bucket (buckets blockIdx.x, + gridDim.x, ...):
-//  1. the bucket's (raq, index) keys and record positions into shared memory
-//     in zone order (zone counts, their scan, shared-memory cursors);
-//  2. the zone offsets of the bucket's zones (zone_off);
-//  3. each zone of at most kWarpZone objects ranked by one warp and written out
-//     as the segment's SoA, its records gathered from the bucket (read a second
-//     time, from L2); larger zones are copied in zone order to recs_z and
-//     listed for zs_block.
-// A bucket of more than kBucketCap records orders its records through recs_z in
-// global memory instead of shared memory.
+// Pass 3, one block per bucket (buckets blockIdx.x, + gridDim.x, ...).
+// A bucket of at most kBucketCap records is ordered in shared memory by one
+// counting sort over (zone, raq sub-range) bins -- kSubBits leading raq bits,
+// 128 sub-ranges of the turn per zone, 4096 bins per bucket of 32 zones:
+//  1. the bucket's (raq, input index) keys read once, kBucketBatch loads in
+//     flight per thread, into shared memory by bucket position; each key's
+//     slot inside its bin from the bin count's atomic (few keys per bin, so
+//     few collide);
+//  2. the exclusive scan of the bin counts by the block: bin bases, which give
+//     the zone offsets (zone_off) and the zones' bin index rows directly;
+//  3. the bucket positions into bin order (base + slot; shared memory only);
+//  4. each key ranked inside its bin (about one key per bin in a zone of 100
+//     objects): rank = the key's place in the bucket's order;
+//  5. the whole block writes the bucket's SoA in that order, gathering each
+//     record from the bucket a second time (from L2).
+// Zones of more than kWarpZone objects are copied to recs_z in bin order and
+// listed for zs_block.  A bucket of more than kBucketCap records orders its
+// records through recs_z in global memory, one warp per zone (zs_rank).
 constexpr int kBucketCap = 6144;
 constexpr uint16_t kNoRecord = 0xFFFF;   // a position of a zone sorted by zs_block
 constexpr int kBucketWarps = kBucketThreads / 32;
+constexpr int kBucketBatch = 4;          // global loads in flight per thread
+constexpr int kSubBits = 7;
+constexpr int kBinShift = kRaqBits - kSubBits;   // ZRec::raq >> kBinShift = zone in bucket << kSubBits | sub-range
+constexpr int kSortBins = 1 << (kBucketMaxShift + kSubBits);
+constexpr int kBinsPerThread = kSortBins / kBucketThreads;
+static_assert(kBinsPerThread % 4 == 0 && (kSortBins >> kBucketMaxShift) == kBucketThreads / 2,
+              "a zone's bins are owned by 8 threads of 16 bins each");
 
 struct BucketSmem {
-    unsigned long long key[kBucketCap];
-    uint16_t pos[kBucketCap];
+    unsigned long long key[kBucketCap];   // (ZRec::raq, index) key at each bucket position
+    uint16_t pos[kBucketCap];             // bucket position at each bin-order slot
+    uint16_t out[kBucketCap];             // slot inside its bin at each position, then position at each rank
+    union {
+        struct {
+            alignas(16) uint32_t cur[kSortBins];   // bin counts (read as uint4)
+            uint32_t base[kSortBins + 1];          // bin bases; base[kSortBins] = records placed
+        } b;
+        WarpSort ws[kBucketWarps];                 // buckets above kBucketCap
+    } u;
     uint32_t zcnt[1 << kBucketMaxShift];
     uint32_t zbeg[(1 << kBucketMaxShift) + 1];
     uint32_t zcur[1 << kBucketMaxShift];
-    WarpSort ws[kBucketWarps];
+    uint32_t wsum[kBucketWarps];
 };
+
+// Zone offsets of the bucket and the list of its zones for zs_block, from
+// S.zbeg (warp 0).
+__device__ __forceinline__ void zs_zone_offsets(const BucketSmem &S, int bk, int n_buckets, int z0, int nzb,
+                                                uint32_t r0, uint32_t r1, uint32_t *zone_off, int n_zones,
+                                                uint32_t *big, uint32_t *misc)
+{
+    const unsigned lane = threadIdx.x;
+    const uint32_t c = (int)lane < nzb ? S.zbeg[lane + 1] - S.zbeg[lane] : 0u;
+    if ((int)lane < nzb) {
+        zone_off[z0 + lane] = r0 + S.zbeg[lane];
+        if (c > (uint32_t)kWarpZone) {
+            big[atomicAdd(&misc[3], 1u)] = (uint32_t)(z0 + lane);
+            atomicMax(&misc[4], c);
+        }
+    }
+    if (bk == n_buckets - 1 && lane == 0) {
+        zone_off[n_zones] = r1;
+        zone_off[n_zones + 1] = misc[2];
+    }
+}
+
+// A bucket of m <= kBucketCap records (steps 1-5 above).
+__device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__restrict__ rb, ZRec *__restrict__ rz,
+                                               uint32_t m, int bk, int n_buckets, int z0, int nzb, uint32_t r0,
+                                               uint32_t r1, uint32_t *zone_off, int n_zones, const ZOut &o,
+                                               uint32_t *big, uint32_t *misc)
+{
+    const unsigned t = threadIdx.x, lane = t & 31;
+    const int warp = t >> 5;
+    uint32_t *cnt = S.u.b.cur, *base = S.u.b.base;
+    for (int b = t; b < kSortBins; b += kBucketThreads) cnt[b] = 0;
+    __syncthreads();
+    for (uint32_t i0 = t; i0 < m; i0 += kBucketBatch * kBucketThreads) {   // 1. keys and slots
+        uint4 v[kBucketBatch];
+#pragma unroll
+        for (int u = 0; u < kBucketBatch; ++u) {
+            const uint32_t i = i0 + u * kBucketThreads;
+            if (i < m) v[u] = __ldg(reinterpret_cast<const uint4 *>(rb + i) + 1);
+        }
+#pragma unroll
+        for (int u = 0; u < kBucketBatch; ++u) {
+            const uint32_t i = i0 + u * kBucketThreads;
+            if (i >= m) break;
+            S.key[i] = ((unsigned long long)v[u].z << 32) | v[u].w;
+            if ((v[u].z >> kRaqBits) < (uint32_t)nzb) S.out[i] = (uint16_t)atomicAdd(&cnt[v[u].z >> kBinShift], 1u);
+            else {
+                S.out[i] = kNoRecord;
+                atomicOr(&misc[5], 1u);   // cannot happen: written by zc_scatter for this bucket
+            }
+        }
+    }
+    __syncthreads();
+    {   // 2. exclusive scan; thread t owns bins [kBinsPerThread t, kBinsPerThread (t + 1))
+        uint32_t c[kBinsPerThread], tot = 0;
+#pragma unroll
+        for (int j = 0; j < kBinsPerThread; j += 4) {
+            const uint4 v = reinterpret_cast<const uint4 *>(cnt + kBinsPerThread * t)[j / 4];
+            c[j] = v.x;
+            c[j + 1] = v.y;
+            c[j + 2] = v.z;
+            c[j + 3] = v.w;
+            tot += v.x + v.y + v.z + v.w;
+        }
+        uint32_t incl = tot;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (unsigned)d) incl += y;
+        }
+        if (lane == 31) S.wsum[warp] = incl;
+        __syncthreads();
+        uint32_t run = incl - tot;
+        for (int w = 0; w < warp; ++w) run += S.wsum[w];
+        if ((t & 7) == 0) S.zbeg[t >> 3] = run;   // zone t / 8 begins at bin kBinsPerThread t
+#pragma unroll
+        for (int j = 0; j < kBinsPerThread; ++j) {
+            base[kBinsPerThread * t + j] = run;
+            run += c[j];
+        }
+        if (t == kBucketThreads - 1) {
+            base[kSortBins] = run;
+            S.zbeg[1 << kBucketMaxShift] = run;
+        }
+    }
+    __syncthreads();
+    if (t < 32) zs_zone_offsets(S, bk, n_buckets, z0, nzb, r0, r1, zone_off, n_zones, big, misc);
+    if (o.zbin) {   // row j of zone zl: start of bin j + 1 inside the zone
+        const int L = o.bin_log2;
+        for (int e = t; e < (nzb << L); e += kBucketThreads) {
+            const int zl = e >> L, j = e & ((1 << L) - 1);
+            const uint32_t v = base[(zl << kSubBits) + ((j + 1) << (kSubBits - L))] - base[zl << kSubBits];
+            o.zbin[((size_t)(z0 + zl) << L) + j] = (uint16_t)min(v, 0xFFFFu);
+        }
+    }
+    for (uint32_t i = t; i < m; i += kBucketThreads) {   // 3. positions into bin order
+        const uint16_t sl = S.out[i];
+        if (sl != kNoRecord) S.pos[base[(uint32_t)(S.key[i] >> (32 + kBinShift))] + sl] = (uint16_t)i;
+    }
+    __syncthreads();
+    const uint32_t mc = base[kSortBins];   // records placed (= m)
+    for (uint32_t q = t; q < mc; q += kBucketThreads) {   // 4. ranks inside the bins
+        const uint16_t i = S.pos[q];
+        const unsigned long long k = S.key[i];
+        const uint32_t b = (uint32_t)(k >> (32 + kBinShift)), zl = b >> kSubBits;
+        if (S.zbeg[zl + 1] - S.zbeg[zl] > (uint32_t)kWarpZone) {   // zs_block sorts it from recs_z
+            const ZRec r = zs_load_ro(rb + i);
+            st_rec(rz + q, r.ra, r.dec, (unsigned long long)r.id, r.raq, r.idx);
+            S.out[q] = kNoRecord;
+            continue;
+        }
+        // keys are distinct (the input index is part of them); an equal key would
+        // count by its slot, so the ranks stay a permutation whatever the keys
+        const uint32_t b0 = base[b], b1 = base[b + 1];
+        uint32_t rank = b0;
+        for (uint32_t p = b0; p < b1; ++p) {
+            const unsigned long long kp = S.key[S.pos[p]];
+            rank += (kp < k || (kp == k && p < q)) ? 1u : 0u;
+        }
+        S.out[rank] = i;
+    }
+    __syncthreads();
+    // 5. the bucket's SoA in order, kBucketBatch records per thread in flight: every
+    // lane busy whatever the zone sizes, writes contiguous across zones
+    for (uint32_t j0 = t; j0 < mc; j0 += kBucketBatch * kBucketThreads) {
+        ZRec x[kBucketBatch];
+        uint16_t q[kBucketBatch];
+#pragma unroll
+        for (int u = 0; u < kBucketBatch; ++u) {
+            const uint32_t j = j0 + u * kBucketThreads;
+            q[u] = j < mc ? S.out[j] : kNoRecord;
+            if (q[u] != kNoRecord) x[u] = zs_load_ro(rb + q[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kBucketBatch; ++u)
+            if (q[u] != kNoRecord) zs_emit(x[u], (unsigned long long)r0 + j0 + u * kBucketThreads, o);
+    }
+    __syncthreads();
+}
+
+// A bucket of more than kBucketCap records: zone order through recs_z, then
+// one warp per zone of at most kWarpZone objects ranks and emits it.
+__device__ __forceinline__ void zs_bucket_global(BucketSmem &S, const ZRec *__restrict__ rb, ZRec *__restrict__ rz,
+                                                 uint32_t m, int bk, int n_buckets, int z0, int nzb, uint32_t r0,
+                                                 uint32_t r1, uint32_t *zone_off, int n_zones, const ZOut &o,
+                                                 uint32_t *big, uint32_t *misc)
+{
+    const unsigned t = threadIdx.x, lane = t & 31;
+    const int warp = t >> 5;
+    WarpSort &W = S.u.ws[warp];
+    if (t < 32) S.zcnt[t] = 0;
+    __syncthreads();
+    for (uint32_t i = t; i < m; i += kBucketThreads) {   // zone counts
+        const uint32_t zl = reinterpret_cast<const uint4 *>(rb + i)[1].z >> kRaqBits;
+        if (zl < (uint32_t)nzb) atomicAdd(&S.zcnt[zl], 1u);
+        else atomicOr(&misc[5], 1u);   // cannot happen: written by zc_scatter for this bucket
+    }
+    __syncthreads();
+    if (t < 32) {   // exclusive scan of the (at most 32) zone counts
+        const uint32_t c = (int)t < nzb ? S.zcnt[t] : 0u;
+        uint32_t incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (unsigned)d) incl += y;
+        }
+        S.zbeg[t] = incl - c;
+        S.zcur[t] = incl - c;
+        if (t == 31) S.zbeg[32] = incl;
+        __syncwarp();
+        zs_zone_offsets(S, bk, n_buckets, z0, nzb, r0, r1, zone_off, n_zones, big, misc);
+    }
+    __syncthreads();
+    for (uint32_t i = t; i < m; i += kBucketThreads) {   // records in zone order
+        const ZRec *p = rb + i;
+        const uint4 v = reinterpret_cast<const uint4 *>(p)[1];
+        const uint32_t zl = v.z >> kRaqBits;
+        if (zl >= (uint32_t)nzb) continue;
+        const uint32_t q = atomicAdd(&S.zcur[zl], 1u);
+        reinterpret_cast<double2 *>(rz + q)[0] = reinterpret_cast<const double2 *>(p)[0];
+        reinterpret_cast<uint4 *>(rz + q)[1] = v;
+    }
+    __syncthreads();
+    for (int k = warp; k < nzb; k += kBucketWarps) {
+        const uint32_t zb = S.zbeg[k], mz = S.zbeg[k + 1] - zb;
+        const ZRec *zr = rz + zb;
+        if (o.zbin)   // the zone's bin index (the order inside the zone does not matter)
+            zone_bins_warp(mz, [&](uint32_t q) { return (uint32_t)(zrec_key(zr + q) >> 32); }, W.hist,
+                           o.zbin + ((size_t)(z0 + k) << o.bin_log2), o.bin_log2, lane);
+        if (mz == 0 || mz > (uint32_t)kWarpZone) continue;   // zs_block sorts a large zone from recs_z
+        zs_rank(mz, [&](uint32_t q) { return zrec_key(zr + q); }, W, lane);
+        for (uint32_t p = lane; p < mz; p += 32)
+            zs_emit(zs_load(zr + W.at[p]), (unsigned long long)r0 + zb + p, o);
+        __syncwarp();
+    }
+    __syncthreads();
+}
 
 __global__ void __launch_bounds__(kBucketThreads, 2)
 zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint32_t *__restrict__ bend,
@@ -808,125 +1028,17 @@ zs_bucket(const ZRec *__restrict__ recs_b, ZRec *__restrict__ recs_z, const uint
 {
     extern __shared__ __align__(16) unsigned char bk_smem[];
     BucketSmem &S = *reinterpret_cast<BucketSmem *>(bk_smem);
-    const unsigned lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    WarpSort &W = S.ws[warp];
     for (int bk = blockIdx.x; bk < n_buckets; bk += gridDim.x) {
         const int z0 = bk << shift;
         const int nzb = min(1 << shift, n_zones - z0);
         const uint32_t r0 = bk ? bend[bk - 1] : 0u, r1 = bend[bk];
         const uint32_t m = r1 - r0;
-        if (threadIdx.x < 32) S.zcnt[threadIdx.x] = 0;
-        __syncthreads();
-        // zone counts
-        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-            const uint32_t zl = reinterpret_cast<const uint4 *>(recs_b + r0 + i)[1].z >> kRaqBits;
-            if (zl < (uint32_t)nzb) atomicAdd(&S.zcnt[zl], 1u);
-            else atomicOr(&misc[5], 1u);   // cannot happen: written by zc_scatter for this bucket
-        }
-        __syncthreads();
-        if (threadIdx.x < 32) {   // exclusive scan of the (at most 32) zone counts
-            const uint32_t c = (int)threadIdx.x < nzb ? S.zcnt[threadIdx.x] : 0u;
-            uint32_t incl = c;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= (unsigned)d) incl += y;
-            }
-            S.zbeg[threadIdx.x] = incl - c;
-            S.zcur[threadIdx.x] = incl - c;
-            if (threadIdx.x == 31) S.zbeg[32] = incl;
-            if ((int)threadIdx.x < nzb) {
-                zone_off[z0 + threadIdx.x] = r0 + incl - c;
-                if (c > (uint32_t)kWarpZone) {
-                    big[atomicAdd(&misc[3], 1u)] = (uint32_t)(z0 + threadIdx.x);
-                    atomicMax(&misc[4], c);
-                }
-            }
-            if (bk == n_buckets - 1 && threadIdx.x == 0) {
-                zone_off[n_zones] = r1;
-                zone_off[n_zones + 1] = misc[2];
-            }
-        }
-        __syncthreads();
-        const bool in_smem = m <= (uint32_t)kBucketCap;
-        // keys (and positions) in zone order
-        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-            const ZRec *p = recs_b + r0 + i;
-            const uint4 t = reinterpret_cast<const uint4 *>(p)[1];
-            const uint32_t zl = t.z >> kRaqBits;
-            if (zl >= (uint32_t)nzb) continue;
-            const uint32_t q = atomicAdd(&S.zcur[zl], 1u);
-            if (in_smem) {
-                S.key[q] = ((unsigned long long)(t.z & kRaqMask) << 32) | t.w;
-                S.pos[q] = (uint16_t)i;
-            } else {
-                const double2 a = reinterpret_cast<const double2 *>(p)[0];
-                reinterpret_cast<double2 *>(recs_z + r0 + q)[0] = a;
-                reinterpret_cast<uint4 *>(recs_z + r0 + q)[1] = t;
-            }
-        }
-        __syncthreads();
-        for (int k = warp; k < nzb; k += kBucketWarps) {
-            const uint32_t zb = S.zbeg[k], mz = S.zbeg[k + 1] - zb;
-            if (o.zbin) {   // the zone's bin index (the order inside the zone does not matter)
-                uint16_t *row = o.zbin + ((size_t)(z0 + k) << o.bin_log2);
-                if (in_smem)
-                    zone_bins_warp(mz, [&](uint32_t q) { return (uint32_t)(S.key[zb + q] >> 32); }, W.hist, row,
-                                   o.bin_log2, lane);
-                else
-                    zone_bins_warp(mz, [&](uint32_t q) { return (uint32_t)(zrec_key(recs_z + r0 + zb + q) >> 32); },
-                                   W.hist, row, o.bin_log2, lane);
-            }
-            if (mz == 0) continue;
-            if (mz > (uint32_t)kWarpZone) {   // zs_block sorts it from recs_z
-                if (in_smem)
-                    for (uint32_t q = lane; q < mz; q += 32) {
-                        const ZRec r = zs_load_ro(recs_b + r0 + S.pos[zb + q]);
-                        st_rec(recs_z + r0 + zb + q, r.ra, r.dec, (unsigned long long)r.id, r.raq, r.idx);
-                        S.pos[zb + q] = kNoRecord;   // not written by the bucket's emit below
-                    }
-                continue;
-            }
-            if (in_smem) {
-                // the zone's records in sorted order: pos[zb + p] = bucket position of rank p
-                zs_rank(mz, [&](uint32_t q) { return S.key[zb + q]; }, W, lane);
-                uint16_t v[kWarpZone / 32];
-#pragma unroll
-                for (int e = 0; e < kWarpZone / 32; ++e) {
-                    const uint32_t p = lane + 32u * e;
-                    v[e] = p < mz ? S.pos[zb + W.at[p]] : (uint16_t)0;
-                }
-                __syncwarp();
-#pragma unroll
-                for (int e = 0; e < kWarpZone / 32; ++e) {
-                    const uint32_t p = lane + 32u * e;
-                    if (p < mz) S.pos[zb + p] = v[e];
-                }
-            } else {
-                const ZRec *zr = recs_z + r0 + zb;
-                zs_rank(mz, [&](uint32_t q) { return zrec_key(zr + q); }, W, lane);
-                for (uint32_t p = lane; p < mz; p += 32)
-                    zs_emit(zs_load(zr + W.at[p]), (unsigned long long)r0 + zb + p, o);
-            }
-            __syncwarp();
-        }
-        __syncthreads();
-        if (in_smem) {
-            // the whole block writes the bucket's SoA in order, two records per thread in
-            // flight: every lane busy whatever the zone sizes, writes contiguous across zones
-            const uint32_t mc = S.zbeg[32];   // records placed in the bucket's zones (= m)
-            for (uint32_t j = threadIdx.x; j < mc; j += 2 * blockDim.x) {
-                const uint32_t j2 = j + blockDim.x;
-                const uint16_t q1 = S.pos[j], q2 = j2 < mc ? S.pos[j2] : kNoRecord;
-                ZRec r1, r2;
-                if (q1 != kNoRecord) r1 = zs_load_ro(recs_b + r0 + q1);
-                if (q2 != kNoRecord) r2 = zs_load_ro(recs_b + r0 + q2);
-                if (q1 != kNoRecord) zs_emit(r1, (unsigned long long)r0 + j, o);
-                if (q2 != kNoRecord) zs_emit(r2, (unsigned long long)r0 + j2, o);
-            }
-            __syncthreads();
-        }
+        if (m <= (uint32_t)kBucketCap)
+            zs_bucket_smem(S, recs_b + r0, recs_z + r0, m, bk, n_buckets, z0, nzb, r0, r1, zone_off, n_zones, o,
+                           big, misc);
+        else
+            zs_bucket_global(S, recs_b + r0, recs_z + r0, m, bk, n_buckets, z0, nzb, r0, r1, zone_off, n_zones, o,
+                             big, misc);
     }
 }
 
