@@ -346,6 +346,46 @@ def test_crossmatch_streams_a_in_chunks(ctx, fixtures, monkeypatch):
     assert np.array_equal(q, po)
 
 
+def test_crossmatch_dense_chunks(ctx, monkeypatch):
+    # a dense patch streamed in 4,000-object chunks of A with about 9 matches per
+    # object: each chunk's ~36,000 matches written into the caller's pinned buffers
+    # after those of the chunks before it
+    import torch
+    from xmatch_b200 import synth
+    monkeypatch.setenv("XMATCH_CHUNK_OBJS", "4000")
+    rng = np.random.default_rng(41)
+    n = 20_000
+    A = synth.make_objs(np.arange(n, dtype=np.int64), rng.uniform(10.0, 10.2, n), rng.uniform(-0.1, 0.1, n))
+    B = synth.make_objs(np.arange(n, dtype=np.int64) + 10**9, rng.uniform(10.0, 10.2, n), rng.uniform(-0.1, 0.1, n))
+    r = 30 * ARCSEC
+    po, do, _ = oracle.xmatch(A, B, r)
+    po, do = sp(po, do)
+    assert len(po) > 5 * (2 * 4000 + 1024)
+    cap = len(po) + 10
+    P = torch.empty(cap * 2, dtype=torch.int64, pin_memory=True).numpy().reshape(-1, 2)
+    D = torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy()
+    p, d, st = ctx.crossmatch(A, B, r, out=(P, D))
+    p, d = sp(p, d)
+    assert np.array_equal(p, po) and np.max(np.abs(d - do), initial=0) <= DIST_TOL
+    assert st["n_match"] == len(po)
+
+
+def test_crossmatch_config1_mixture_4M(ctx):
+    # one call from pinned host records to pinned host pairs, 4.5M objects a side of
+    # the config-1 mixture (clusters, wrap and polar sources)
+    import torch
+    from xmatch_b200 import synth
+    A, B = synth.config1(n=4_500_000, seed=23)
+    r = ARCSEC
+    po, _, _ = oracle.xmatch(A, B, r, r)
+    po = sp(po)
+    cap = len(po) + 10
+    P = torch.empty(cap * 2, dtype=torch.int64, pin_memory=True).numpy().reshape(-1, 2)
+    p, _, st = ctx.crossmatch(A, B, r, zh_deg=r, with_dist=False, out=(P, None))
+    assert np.array_equal(sp(p), po)
+    assert st["n_match"] == len(po)
+
+
 def test_segmentation_invariance(ctx, fixtures):
     a, _ = fixtures
     whole, _, _ = oracle.xmatch(a, a, 5 * ARCSEC)

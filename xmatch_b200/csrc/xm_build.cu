@@ -804,8 +804,12 @@ constexpr int kSubBits = 7;
 constexpr int kBinShift = kRaqBits - kSubBits;   // ZRec::raq >> kBinShift = zone in bucket << kSubBits | sub-range
 constexpr int kSortBins = 1 << (kBucketMaxShift + kSubBits);
 constexpr int kBinsPerThread = kSortBins / kBucketThreads;
-static_assert(kBinsPerThread % 4 == 0 && (kSortBins >> kBucketMaxShift) == kBucketThreads / 2,
+static_assert(kBinsPerThread == 16 && (kSortBins >> kBucketMaxShift) == kBucketThreads / 2,
               "a zone's bins are owned by 8 threads of 16 bins each");
+// Bin b is kept at word b + b / 16: the 16 bins a thread scans start 17 words
+// apart, so the 32 lanes of a warp touch 32 different banks.
+constexpr int kPaddedBins = kSortBins + kSortBins / 16;
+__device__ __forceinline__ uint32_t bin_word(uint32_t b) { return b + (b >> 4); }
 
 struct BucketSmem {
     unsigned long long key[kBucketCap];   // (ZRec::raq, index) key at each bucket position
@@ -813,8 +817,8 @@ struct BucketSmem {
     uint16_t out[kBucketCap];             // slot inside its bin at each position, then position at each rank
     union {
         struct {
-            alignas(16) uint32_t cur[kSortBins];   // bin counts (read as uint4)
-            uint32_t base[kSortBins + 1];          // bin bases; base[kSortBins] = records placed
+            uint32_t cnt[kPaddedBins];        // bin counts, at bin_word(b)
+            uint32_t base[kPaddedBins + 1];   // bin bases, at bin_word(b); bin_word(kSortBins) = records placed
         } b;
         WarpSort ws[kBucketWarps];                 // buckets above kBucketCap
     } u;
@@ -853,8 +857,8 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
 {
     const unsigned t = threadIdx.x, lane = t & 31;
     const int warp = t >> 5;
-    uint32_t *cnt = S.u.b.cur, *base = S.u.b.base;
-    for (int b = t; b < kSortBins; b += kBucketThreads) cnt[b] = 0;
+    uint32_t *cnt = S.u.b.cnt, *base = S.u.b.base;
+    for (int b = t; b < kPaddedBins; b += kBucketThreads) cnt[b] = 0;
     __syncthreads();
     for (uint32_t i0 = t; i0 < m; i0 += kBucketBatch * kBucketThreads) {   // 1. keys and slots
         uint4 v[kBucketBatch];
@@ -868,7 +872,7 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
             const uint32_t i = i0 + u * kBucketThreads;
             if (i >= m) break;
             S.key[i] = ((unsigned long long)v[u].z << 32) | v[u].w;
-            if ((v[u].z >> kRaqBits) < (uint32_t)nzb) S.out[i] = (uint16_t)atomicAdd(&cnt[v[u].z >> kBinShift], 1u);
+            if ((v[u].z >> kRaqBits) < (uint32_t)nzb) S.out[i] = (uint16_t)atomicAdd(&cnt[bin_word(v[u].z >> kBinShift)], 1u);
             else {
                 S.out[i] = kNoRecord;
                 atomicOr(&misc[5], 1u);   // cannot happen: written by zc_scatter for this bucket
@@ -879,13 +883,9 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
     {   // 2. exclusive scan; thread t owns bins [kBinsPerThread t, kBinsPerThread (t + 1))
         uint32_t c[kBinsPerThread], tot = 0;
 #pragma unroll
-        for (int j = 0; j < kBinsPerThread; j += 4) {
-            const uint4 v = reinterpret_cast<const uint4 *>(cnt + kBinsPerThread * t)[j / 4];
-            c[j] = v.x;
-            c[j + 1] = v.y;
-            c[j + 2] = v.z;
-            c[j + 3] = v.w;
-            tot += v.x + v.y + v.z + v.w;
+        for (int j = 0; j < kBinsPerThread; ++j) {
+            c[j] = cnt[(kBinsPerThread + 1) * t + j];   // bin_word(kBinsPerThread t + j)
+            tot += c[j];
         }
         uint32_t incl = tot;
 #pragma unroll
@@ -900,11 +900,11 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
         if ((t & 7) == 0) S.zbeg[t >> 3] = run;   // zone t / 8 begins at bin kBinsPerThread t
 #pragma unroll
         for (int j = 0; j < kBinsPerThread; ++j) {
-            base[kBinsPerThread * t + j] = run;
+            base[(kBinsPerThread + 1) * t + j] = run;
             run += c[j];
         }
         if (t == kBucketThreads - 1) {
-            base[kSortBins] = run;
+            base[bin_word(kSortBins)] = run;
             S.zbeg[1 << kBucketMaxShift] = run;
         }
     }
@@ -914,16 +914,17 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
         const int L = o.bin_log2;
         for (int e = t; e < (nzb << L); e += kBucketThreads) {
             const int zl = e >> L, j = e & ((1 << L) - 1);
-            const uint32_t v = base[(zl << kSubBits) + ((j + 1) << (kSubBits - L))] - base[zl << kSubBits];
+            const uint32_t v =
+                base[bin_word((zl << kSubBits) + ((j + 1) << (kSubBits - L)))] - base[bin_word(zl << kSubBits)];
             o.zbin[((size_t)(z0 + zl) << L) + j] = (uint16_t)min(v, 0xFFFFu);
         }
     }
     for (uint32_t i = t; i < m; i += kBucketThreads) {   // 3. positions into bin order
         const uint16_t sl = S.out[i];
-        if (sl != kNoRecord) S.pos[base[(uint32_t)(S.key[i] >> (32 + kBinShift))] + sl] = (uint16_t)i;
+        if (sl != kNoRecord) S.pos[base[bin_word((uint32_t)(S.key[i] >> (32 + kBinShift)))] + sl] = (uint16_t)i;
     }
     __syncthreads();
-    const uint32_t mc = base[kSortBins];   // records placed (= m)
+    const uint32_t mc = base[bin_word(kSortBins)];   // records placed (= m)
     for (uint32_t q = t; q < mc; q += kBucketThreads) {   // 4. ranks inside the bins
         const uint16_t i = S.pos[q];
         const unsigned long long k = S.key[i];
@@ -936,7 +937,7 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
         }
         // keys are distinct (the input index is part of them); an equal key would
         // count by its slot, so the ranks stay a permutation whatever the keys
-        const uint32_t b0 = base[b], b1 = base[b + 1];
+        const uint32_t b0 = base[bin_word(b)], b1 = base[bin_word(b + 1)];
         uint32_t rank = b0;
         for (uint32_t p = b0; p < b1; ++p) {
             const unsigned long long kp = S.key[S.pos[p]];
