@@ -782,15 +782,16 @@ __device__ __forceinline__ void zs_rank(uint32_t m, K key_of, WarpSort &W, unsig
 // A bucket of at most kBucketCap records is ordered in shared memory by one
 // counting sort over (zone, raq sub-range) bins -- kSubBits leading raq bits,
 // 128 sub-ranges of the turn per zone, 4096 bins per bucket of 32 zones:
-//  1. the bucket's (raq, input index) keys read once, kBucketBatch loads in
-//     flight per thread, into shared memory by bucket position; each key's
-//     slot inside its bin from the bin count's atomic (few keys per bin, so
-//     few collide);
+//  1. the bucket's keys (ZRec::raq: zone in bucket, raq) read once,
+//     kKeyBatch loads in flight per thread, into shared memory by bucket
+//     position; each key's slot inside its bin from the bin count's atomic
+//     (few keys per bin, so few collide);
 //  2. the exclusive scan of the bin counts by the block: bin bases, which give
 //     the zone offsets (zone_off) and the zones' bin index rows directly;
 //  3. the bucket positions into bin order (base + slot; shared memory only);
-//  4. each key ranked inside its bin (about one key per bin in a zone of 100
-//     objects): rank = the key's place in the bucket's order;
+//  4. each key ranked inside its bin by raq, then by input index (read from
+//     the records when two raq are equal; about one key per bin in a zone of
+//     100 objects): rank = the key's place in the bucket's order;
 //  5. the whole block writes the bucket's SoA in that order, gathering each
 //     record from the bucket a second time (from L2).
 // Zones of more than kWarpZone objects are copied to recs_z in bin order and
@@ -799,29 +800,39 @@ __device__ __forceinline__ void zs_rank(uint32_t m, K key_of, WarpSort &W, unsig
 constexpr int kBucketCap = 6144;
 constexpr uint16_t kNoRecord = 0xFFFF;   // a position of a zone sorted by zs_block
 constexpr int kBucketWarps = kBucketThreads / 32;
-constexpr int kBucketBatch = 4;          // global loads in flight per thread
+constexpr int kKeyBatch = 8;             // key loads in flight per thread (step 1)
+constexpr int kEmitBatch = 2;            // record loads in flight per thread (step 5)
 constexpr int kSubBits = 7;
 constexpr int kBinShift = kRaqBits - kSubBits;   // ZRec::raq >> kBinShift = zone in bucket << kSubBits | sub-range
 constexpr int kSortBins = 1 << (kBucketMaxShift + kSubBits);
 constexpr int kBinsPerThread = kSortBins / kBucketThreads;
 static_assert(kBinsPerThread == 16 && (kSortBins >> kBucketMaxShift) == kBucketThreads / 2,
               "a zone's bins are owned by 8 threads of 16 bins each");
-// Bin b is kept at word b + b / 16: the 16 bins a thread scans start 17 words
-// apart, so the 32 lanes of a warp touch 32 different banks.
-constexpr int kPaddedBins = kSortBins + kSortBins / 16;
-__device__ __forceinline__ uint32_t bin_word(uint32_t b) { return b + (b >> 4); }
+// Bin counts and bases are 16-bit (a bucket holds at most kBucketCap records),
+// two bins to a word; bin b is in half b & 1 of word b / 2 + b / 16: the 8
+// words of a thread's 16 bins start 9 words apart, so the 32 lanes of a warp
+// touch 32 different banks.
+constexpr int kBinWords = kSortBins / 2 + kSortBins / 16;   // bins 0 .. kSortBins - 1
+__device__ __forceinline__ uint32_t bin_word(uint32_t b) { return (b >> 1) + (b >> 4); }
+__device__ __forceinline__ uint32_t bin_get(const uint32_t *w, uint32_t b)
+{
+    return (w[bin_word(b)] >> ((b & 1u) << 4)) & 0xFFFFu;
+}
+static_assert(kBucketCap < 0x10000, "16-bit bin counts and bases");
 
+// 66 KB (two blocks per SM; three, with the 80 registers a thread that allows, measured
+// slower: 1.75 against 1.55 ms at 50M).
 struct BucketSmem {
-    unsigned long long key[kBucketCap];   // (ZRec::raq, index) key at each bucket position
-    uint16_t pos[kBucketCap];             // bucket position at each bin-order slot
-    uint16_t out[kBucketCap];             // slot inside its bin at each position, then position at each rank
     union {
         struct {
-            uint32_t cnt[kPaddedBins];        // bin counts, at bin_word(b)
-            uint32_t base[kPaddedBins + 1];   // bin bases, at bin_word(b); bin_word(kSortBins) = records placed
-        } b;
-        WarpSort ws[kBucketWarps];                 // buckets above kBucketCap
+            uint32_t key[kBucketCap];   // ZRec::raq (zone in bucket, raq) at each bucket position
+            uint16_t pos[kBucketCap];   // bucket position at each bin-order slot
+            uint16_t out[kBucketCap];   // slot inside its bin at each position, then position at each rank
+        } s;
+        WarpSort ws[kBucketWarps];      // buckets above kBucketCap
     } u;
+    uint32_t cnt[kBinWords];            // bin counts (bin_get)
+    uint32_t base[kBinWords + 1];       // bin bases (bin_get); bin kSortBins = records placed
     uint32_t zcnt[1 << kBucketMaxShift];
     uint32_t zbeg[(1 << kBucketMaxShift) + 1];
     uint32_t zcur[1 << kBucketMaxShift];
@@ -857,35 +868,40 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
 {
     const unsigned t = threadIdx.x, lane = t & 31;
     const int warp = t >> 5;
-    uint32_t *cnt = S.u.b.cnt, *base = S.u.b.base;
-    for (int b = t; b < kPaddedBins; b += kBucketThreads) cnt[b] = 0;
+    uint32_t *key = S.u.s.key;
+    uint16_t *pos = S.u.s.pos, *out = S.u.s.out;
+    for (int w = t; w < kBinWords; w += kBucketThreads) S.cnt[w] = 0;
     __syncthreads();
-    for (uint32_t i0 = t; i0 < m; i0 += kBucketBatch * kBucketThreads) {   // 1. keys and slots
-        uint4 v[kBucketBatch];
+    for (uint32_t i0 = t; i0 < m; i0 += kKeyBatch * kBucketThreads) {   // 1. keys and slots
+        uint32_t v[kKeyBatch];
 #pragma unroll
-        for (int u = 0; u < kBucketBatch; ++u) {
+        for (int u = 0; u < kKeyBatch; ++u) {
             const uint32_t i = i0 + u * kBucketThreads;
-            if (i < m) v[u] = __ldg(reinterpret_cast<const uint4 *>(rb + i) + 1);
+            if (i < m) v[u] = __ldg(&rb[i].raq);
         }
 #pragma unroll
-        for (int u = 0; u < kBucketBatch; ++u) {
+        for (int u = 0; u < kKeyBatch; ++u) {
             const uint32_t i = i0 + u * kBucketThreads;
             if (i >= m) break;
-            S.key[i] = ((unsigned long long)v[u].z << 32) | v[u].w;
-            if ((v[u].z >> kRaqBits) < (uint32_t)nzb) S.out[i] = (uint16_t)atomicAdd(&cnt[bin_word(v[u].z >> kBinShift)], 1u);
-            else {
-                S.out[i] = kNoRecord;
+            key[i] = v[u];
+            if ((v[u] >> kRaqBits) < (uint32_t)nzb) {
+                const uint32_t b = v[u] >> kBinShift, sh = (b & 1u) << 4;
+                out[i] = (uint16_t)(atomicAdd(&S.cnt[bin_word(b)], 1u << sh) >> sh);
+            } else {
+                out[i] = kNoRecord;
                 atomicOr(&misc[5], 1u);   // cannot happen: written by zc_scatter for this bucket
             }
         }
     }
     __syncthreads();
-    {   // 2. exclusive scan; thread t owns bins [kBinsPerThread t, kBinsPerThread (t + 1))
-        uint32_t c[kBinsPerThread], tot = 0;
+    {   // 2. exclusive scan; thread t owns bins [kBinsPerThread t, kBinsPerThread (t + 1)),
+        //    words [9 t, 9 t + 8) of S.cnt and S.base
+        constexpr int W = kBinsPerThread / 2;
+        uint32_t c[W], tot = 0;
 #pragma unroll
-        for (int j = 0; j < kBinsPerThread; ++j) {
-            c[j] = cnt[(kBinsPerThread + 1) * t + j];   // bin_word(kBinsPerThread t + j)
-            tot += c[j];
+        for (int j = 0; j < W; ++j) {
+            c[j] = S.cnt[(W + 1) * t + j];
+            tot += (c[j] & 0xFFFFu) + (c[j] >> 16);
         }
         uint32_t incl = tot;
 #pragma unroll
@@ -899,12 +915,13 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
         for (int w = 0; w < warp; ++w) run += S.wsum[w];
         if ((t & 7) == 0) S.zbeg[t >> 3] = run;   // zone t / 8 begins at bin kBinsPerThread t
 #pragma unroll
-        for (int j = 0; j < kBinsPerThread; ++j) {
-            base[(kBinsPerThread + 1) * t + j] = run;
-            run += c[j];
+        for (int j = 0; j < W; ++j) {
+            const uint32_t lo = run, hi = run + (c[j] & 0xFFFFu);
+            S.base[(W + 1) * t + j] = lo | (hi << 16);
+            run = hi + (c[j] >> 16);
         }
         if (t == kBucketThreads - 1) {
-            base[bin_word(kSortBins)] = run;
+            S.base[bin_word(kSortBins)] = run;
             S.zbeg[1 << kBucketMaxShift] = run;
         }
     }
@@ -914,51 +931,58 @@ __device__ __forceinline__ void zs_bucket_smem(BucketSmem &S, const ZRec *__rest
         const int L = o.bin_log2;
         for (int e = t; e < (nzb << L); e += kBucketThreads) {
             const int zl = e >> L, j = e & ((1 << L) - 1);
-            const uint32_t v =
-                base[bin_word((zl << kSubBits) + ((j + 1) << (kSubBits - L)))] - base[bin_word(zl << kSubBits)];
-            o.zbin[((size_t)(z0 + zl) << L) + j] = (uint16_t)min(v, 0xFFFFu);
+            const uint32_t v = bin_get(S.base, (zl << kSubBits) + ((j + 1) << (kSubBits - L))) -
+                               bin_get(S.base, zl << kSubBits);
+            o.zbin[((size_t)(z0 + zl) << L) + j] = (uint16_t)v;
         }
     }
     for (uint32_t i = t; i < m; i += kBucketThreads) {   // 3. positions into bin order
-        const uint16_t sl = S.out[i];
-        if (sl != kNoRecord) S.pos[base[bin_word((uint32_t)(S.key[i] >> (32 + kBinShift)))] + sl] = (uint16_t)i;
+        const uint16_t sl = out[i];
+        if (sl != kNoRecord) pos[bin_get(S.base, key[i] >> kBinShift) + sl] = (uint16_t)i;
     }
     __syncthreads();
-    const uint32_t mc = base[bin_word(kSortBins)];   // records placed (= m)
+    const uint32_t mc = bin_get(S.base, kSortBins);   // records placed (= m)
     for (uint32_t q = t; q < mc; q += kBucketThreads) {   // 4. ranks inside the bins
-        const uint16_t i = S.pos[q];
-        const unsigned long long k = S.key[i];
-        const uint32_t b = (uint32_t)(k >> (32 + kBinShift)), zl = b >> kSubBits;
+        const uint16_t i = pos[q];
+        const uint32_t k = key[i];
+        const uint32_t b = k >> kBinShift, zl = b >> kSubBits;
         if (S.zbeg[zl + 1] - S.zbeg[zl] > (uint32_t)kWarpZone) {   // zs_block sorts it from recs_z
             const ZRec r = zs_load_ro(rb + i);
             st_rec(rz + q, r.ra, r.dec, (unsigned long long)r.id, r.raq, r.idx);
-            S.out[q] = kNoRecord;
+            out[q] = kNoRecord;
             continue;
         }
-        // keys are distinct (the input index is part of them); an equal key would
-        // count by its slot, so the ranks stay a permutation whatever the keys
-        const uint32_t b0 = base[bin_word(b)], b1 = base[bin_word(b + 1)];
+        // order inside the bin: raq, then the input index (read from the records, for
+        // the rare equal raq), then the slot -- the ranks stay a permutation whatever
+        // the keys
+        const uint32_t b0 = bin_get(S.base, b), b1 = bin_get(S.base, b + 1);
         uint32_t rank = b0;
         for (uint32_t p = b0; p < b1; ++p) {
-            const unsigned long long kp = S.key[S.pos[p]];
-            rank += (kp < k || (kp == k && p < q)) ? 1u : 0u;
+            const uint16_t ip = pos[p];
+            const uint32_t kp = key[ip];
+            bool before = kp < k;
+            if (kp == k && p != q) {
+                const uint32_t xp = __ldg(&rb[ip].idx), xq = __ldg(&rb[i].idx);
+                before = xp < xq || (xp == xq && p < q);
+            }
+            rank += before ? 1u : 0u;
         }
-        S.out[rank] = i;
+        out[rank] = i;
     }
     __syncthreads();
-    // 5. the bucket's SoA in order, kBucketBatch records per thread in flight: every
+    // 5. the bucket's SoA in order, kEmitBatch records per thread in flight: every
     // lane busy whatever the zone sizes, writes contiguous across zones
-    for (uint32_t j0 = t; j0 < mc; j0 += kBucketBatch * kBucketThreads) {
-        ZRec x[kBucketBatch];
-        uint16_t q[kBucketBatch];
+    for (uint32_t j0 = t; j0 < mc; j0 += kEmitBatch * kBucketThreads) {
+        ZRec x[kEmitBatch];
+        uint16_t q[kEmitBatch];
 #pragma unroll
-        for (int u = 0; u < kBucketBatch; ++u) {
+        for (int u = 0; u < kEmitBatch; ++u) {
             const uint32_t j = j0 + u * kBucketThreads;
-            q[u] = j < mc ? S.out[j] : kNoRecord;
+            q[u] = j < mc ? out[j] : kNoRecord;
             if (q[u] != kNoRecord) x[u] = zs_load_ro(rb + q[u]);
         }
 #pragma unroll
-        for (int u = 0; u < kBucketBatch; ++u)
+        for (int u = 0; u < kEmitBatch; ++u)
             if (q[u] != kNoRecord) zs_emit(x[u], (unsigned long long)r0 + j0 + u * kBucketThreads, o);
     }
     __syncthreads();
