@@ -58,6 +58,24 @@ def test_idradec_roundtrip(tmp_path, fixtures):
     assert c.tobytes() == a[100:150].tobytes()
     with pytest.raises(xm.XmatchError):
         xm.read_idradec(str(tmp_path / "missing.idradec"))
+    with pytest.raises(xm.XmatchError):   # records beyond the end of the file
+        xm.read_idradec(f, len(a) - 10, 20)
+
+
+def test_idradec_read_in_parallel_pieces(tmp_path):
+    # 200 MB: the reader splits it into 64 MB pieces read by several threads
+    import xmatch_b200 as xm
+    n = 200 * 2 ** 20 // 24 + 5
+    a = np.empty(n, xm.OBJ_DTYPE)
+    a["id"] = np.arange(n, dtype=np.int64) * 7 + 1
+    a["ra"] = np.arange(n, dtype=np.float64) * 1e-5
+    a["dec"] = -np.arange(n, dtype=np.float64) * 1e-6
+    f = str(tmp_path / "big.idradec")
+    a.tofile(f)
+    b = xm.read_idradec(f)
+    assert b.tobytes() == a.tobytes()
+    c = xm.read_idradec(f, 3, n - 4)
+    assert c.tobytes() == a[3 : n - 1].tobytes()
 
 
 def test_pairs_writer_formats(tmp_path):

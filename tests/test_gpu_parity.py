@@ -336,6 +336,14 @@ def test_crossmatch_streams_a_in_chunks(ctx, fixtures, monkeypatch):
         p, d, st = ctx.crossmatch(a, a2, r, out=(P, D))
         p, d = sp(p, d)
         assert np.array_equal(p, po) and np.max(np.abs(d - do), initial=0) <= DIST_TOL
+    # explicit schedules: the largest chunk not the first (the staging slots take
+    # the largest), a chunk of one object, an empty chunk
+    for w in ("1,3,1", "9997,1,2", "1,0.00001,1"):
+        monkeypatch.setenv("XMATCH_CHUNK_WEIGHTS", w)
+        p, d, st = ctx.crossmatch(a, a2, r, out=(P, D))
+        p, d = sp(p, d)
+        assert np.array_equal(p, po) and np.max(np.abs(d - do), initial=0) <= DIST_TOL
+    monkeypatch.delenv("XMATCH_CHUNK_WEIGHTS")
     # room for fewer than all: the whole match reruns into device buffers, the count is reported
     import xmatch_b200 as xm
     with pytest.raises(xm.XmatchError) as e:

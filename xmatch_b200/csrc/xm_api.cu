@@ -977,15 +977,48 @@ static xm_status grow(xm_ctx *ctx, void **p, size_t *have, size_t need)
 // and matched once (XM_ERR_CAPACITY then reports the count and leaves the
 // matches for xm_fetch_pairs).
 namespace {
-// A objects per chunk at least (environment XMATCH_CHUNK_OBJS overrides it).  A chunk is
-// a slice of A's records in input order, so it spans all of A's zones and its match
-// walks all of B's: few large chunks (12M objects: 49 ms at 50M x 50M against 59 ms
-// for one, 53 ms for 6) balance that against the overlap.
+// Chunks of A.  A chunk is a slice of A's records in input order, so it spans
+// all of A's zones and its match walks all of B's: few large chunks balance that
+// against the overlap.  Their sizes fall towards the end, so that the work left
+// after the last chunk's copy (its build, its match and its matches over the
+// link) is short, while every earlier chunk is still matched before the next one
+// has landed: n chunks of relative sizes n + 1, n, ..., 2, n = nA / 10M (5 at
+// 50M: 48.9 ms at 50M x 50M against 50.1 ms for 4 equal chunks and 59 ms for
+// one).  Environment XMATCH_CHUNK_OBJS sets the objects per chunk that fix n,
+// XMATCH_CHUNK_WEIGHTS (comma-separated relative sizes) the whole schedule.
 uint64_t chunk_objs()
 {
     const char *e = std::getenv("XMATCH_CHUNK_OBJS");
     const unsigned long long v = e ? std::strtoull(e, nullptr, 10) : 0ull;
-    return v ? (uint64_t)v : 12000000ull;   // 4 chunks at 50M: each chunk re-walks B's zones
+    return v ? (uint64_t)v : 10000000ull;
+}
+
+// Chunk boundaries of A: bounds[c] .. bounds[c + 1] is chunk c.
+std::vector<uint64_t> chunk_bounds(uint64_t nA, uint64_t n_chunks)
+{
+    std::vector<double> w;
+    if (const char *e = std::getenv("XMATCH_CHUNK_WEIGHTS")) {
+        for (const char *p = e; *p;) {
+            char *end = nullptr;
+            const double v = std::strtod(p, &end);
+            if (end == p) break;
+            if (v > 0) w.push_back(v);
+            p = *end == ',' ? end + 1 : end;
+        }
+    }
+    if (w.empty()) {
+        for (uint64_t c = 0; c < n_chunks; ++c) w.push_back((double)(n_chunks + 1 - c));
+    }
+    double sum = 0;
+    for (double v : w) sum += v;
+    std::vector<uint64_t> b(1, 0);
+    double acc = 0;
+    for (size_t c = 0; c < w.size(); ++c) {
+        acc += w[c];
+        const uint64_t e = c + 1 == w.size() ? nA : std::min<uint64_t>(nA, (uint64_t)((double)nA * (acc / sum)));
+        b.push_back(std::max(e, b.back()));
+    }
+    return b;
 }
 }
 
@@ -1036,14 +1069,17 @@ extern "C" xm_status xm_crossmatch(xm_ctx *ctx, const xm_obj *A, uint64_t nA, co
         direct.capacity = out->capacity;
     }
     const bool streamed = direct.pairs && (!want_dist || direct.dist);
-    const uint64_t n_chunks = streamed ? std::max<uint64_t>(1, std::min<uint64_t>(16, nA / chunk_objs())) : 1;
-    const uint64_t chunk = n_chunks > 1 ? (nA + n_chunks - 1) / n_chunks : nA;
+    const uint64_t n_even = streamed ? std::max<uint64_t>(1, std::min<uint64_t>(16, nA / chunk_objs())) : 1;
+    const std::vector<uint64_t> bounds = n_even > 1 ? chunk_bounds(nA, n_even) : std::vector<uint64_t>{0, nA};
+    const uint64_t n_chunks = bounds.size() - 1;
+    uint64_t chunk = 0;   // the largest chunk: the size of a staging slot
+    for (uint64_t c = 0; c < n_chunks; ++c) chunk = std::max(chunk, bounds[c + 1] - bounds[c]);
     // A chunks land in two slots of the staging buffer, copied on the second stream
     XM_TRY(grow(ctx, &ctx->stage, &ctx->stage_bytes, 2 * std::max<uint64_t>(chunk, 1) * sizeof(xm_obj)));
     xm_obj *slot[2] = {(xm_obj *)ctx->stage, (xm_obj *)ctx->stage + std::max<uint64_t>(chunk, 1)};
     cudaEvent_t *landed = ctx->ev_slot;   // recorded only here
     auto copy_chunk = [&](uint64_t c) -> xm_status {
-        const uint64_t first = c * chunk, n = std::min<uint64_t>(chunk, nA - first);
+        const uint64_t first = bounds[c], n = bounds[c + 1] - bounds[c];
         if (n) XM_CUDA(ctx, cudaMemcpyAsync(slot[c & 1], A + first, n * sizeof(xm_obj), cudaMemcpyHostToDevice, s2));
         XM_CUDA(ctx, cudaEventRecord(landed[c & 1], s2));
         return XM_OK;
@@ -1069,7 +1105,7 @@ extern "C" xm_status xm_crossmatch(xm_ctx *ctx, const xm_obj *A, uint64_t nA, co
         bool overflow = false;
         rc = new_segment(ctx, 0, zh_deg, &sa);
         for (uint64_t c = 0; rc == XM_OK && c < n_chunks; ++c) {
-            const uint64_t n = std::min<uint64_t>(chunk, nA - std::min<uint64_t>(nA, c * chunk));
+            const uint64_t n = bounds[c + 1] - bounds[c];
             if (cudaStreamWaitEvent(st, landed[c & 1], 0) != cudaSuccess) {
                 rc = XM_ERR_CUDA;
                 break;

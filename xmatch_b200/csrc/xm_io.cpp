@@ -3,9 +3,16 @@
 //              (Obj.h:21-25, read raw by Segment::Load, Segment.cpp:14-22)
 //   pairs    : headerless 16-byte records {int64 idA; int64 idB}
 //              (Worker.cu:407-420), or 24-byte {idA, idB, f64 dist}, or ASCII
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <vector>
+
+#include <fcntl.h>
+#include <unistd.h>
 
 #include "../../include/xmatch.h"
 
@@ -25,18 +32,46 @@ extern "C" xm_status xm_idradec_count(const char *path, uint64_t *n)
     return XM_OK;
 }
 
+// Records [first, first + n) straight into the caller's buffer (pinned memory
+// included) with pread(2) in 64 MB pieces, by up to 8 threads at once for a
+// large read: from the page cache one thread copies a few GB/s, below what the
+// link to the GPU takes.
 extern "C" xm_status xm_idradec_read(const char *path, uint64_t first, uint64_t n, xm_obj *out)
 {
     if (!path || (n && !out)) return XM_ERR_INVALID;
-    FILE *f = std::fopen(path, "rb");
-    if (!f) return XM_ERR_IO;
-    if (fseeko(f, (off_t)(first * sizeof(xm_obj)), SEEK_SET) != 0) {
-        std::fclose(f);
-        return XM_ERR_IO;
+    const int fd = ::open(path, O_RDONLY | O_CLOEXEC);
+    if (fd < 0) return XM_ERR_IO;
+    const uint64_t bytes = n * sizeof(xm_obj);
+    const off_t base = (off_t)(first * sizeof(xm_obj));
+    constexpr uint64_t kPiece = 64ull << 20;
+    const uint64_t pieces = (bytes + kPiece - 1) / kPiece;
+    std::atomic<uint64_t> next{0};
+    std::atomic<bool> ok{true};
+    auto work = [&] {
+        for (uint64_t k; ok.load(std::memory_order_relaxed) && (k = next.fetch_add(1)) < pieces;) {
+            uint64_t done = k * kPiece;
+            const uint64_t end = std::min(bytes, done + kPiece);
+            while (done < end) {
+                const ssize_t r = ::pread(fd, reinterpret_cast<char *>(out) + done, end - done, base + (off_t)done);
+                if (r < 0 && errno == EINTR) continue;
+                if (r <= 0) {   // error, or the file ends before the records asked for
+                    ok = false;
+                    break;
+                }
+                done += (uint64_t)r;
+            }
+        }
+    };
+    const unsigned nt = (unsigned)std::min<uint64_t>(8, pieces);
+    if (nt <= 1) {
+        work();
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned i = 0; i < nt; ++i) th.emplace_back(work);
+        for (auto &t : th) t.join();
     }
-    size_t got = std::fread(out, sizeof(xm_obj), n, f);
-    std::fclose(f);
-    return got == n ? XM_OK : XM_ERR_IO;
+    ::close(fd);
+    return ok ? XM_OK : XM_ERR_IO;
 }
 
 extern "C" xm_status xm_idradec_write(const char *path, const xm_obj *objs, uint64_t n)

@@ -42,11 +42,11 @@
 // predicate with per-pair sincos to every candidate.
 //
 // Output.  Matches are compacted per warp with __ballot_sync/__popc into the
-// warp's buffer in shared memory (idA and the address of idB), which is
-// appended to global memory with one atomicAdd per flush, the idB loads
-// issued under it (Worker.cu:128-240 uses two Hillis-Steele scans per
-// block).  A full output buffer is detected and reported, never silently
-// truncated (Worker.cu:147-148).
+// warp's buffer in shared memory (idA, and the job and index of the B object),
+// which goes to global memory 32 entries at a time: one atomicAdd reserves the
+// slots, the idB loads are issued under it, and the 32 records are stored
+// coalesced (Worker.cu:128-240 uses two Hillis-Steele scans per block).  A full output
+// buffer is detected and reported, never silently truncated (Worker.cu:147-148).
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
@@ -354,7 +354,10 @@ __device__ __forceinline__ int find_job(const JobDev *__restrict__ jobs, int n_j
     return lo;
 }
 
-constexpr int kWarpBuf = 32;
+// Per-warp match buffer: 64 entries, written out 32 at a time.  Each round of
+// phase 2 adds at most 32 matches to a buffer holding fewer than 32, so the
+// staged path never overflows it.
+constexpr int kWarpBuf = 64;
 
 constexpr int kMaxRanges = 9;   // 3 windows x up to 3 zones per lane; beyond that the cursor path
 
@@ -365,20 +368,42 @@ struct WList {
     double alpha[32];
 };
 
-// Per-warp match buffer.  An entry holds idA and the ADDRESS of idB in the B
-// segment; the ids are loaded when the buffer is flushed, all lanes at once
-// and under the output atomic, instead of one dependent load per match.
-struct WBuf {
-    longlong2 ab[kWarpBuf];     // idA, address of idB
-    double d[kWarpBuf];
-    uint32_t job[kWarpBuf];
-    uint32_t count;
+// An entry holds idA and (job << 32 | index of the B object in its segment);
+// idB is loaded when the entry is written out, all lanes at once, instead of
+// one dependent load per match.  Distances are held only by the DIST kernels.
+template <bool DIST>
+struct WBufT {
+    longlong2 ab[kWarpBuf];     // idA, job << 32 | B index
+    double d[DIST ? kWarpBuf : 1];
+    uint32_t count;             // entries [0, min(count, kWarpBuf)) are held; the rest went out directly
 };
 
+// Where B's ids are: in the consumer's current job, or for entries left from a
+// previous tile of a batch, in that job's entry of the job table.
+struct IdSrc {
+    const JobDev *jobs;
+    const JobDev *cur;          // the current job's entry
+    int job;                    // its index
+    __device__ __forceinline__ long long id_of(unsigned long long e) const
+    {
+        const int j = (int)(e >> 32);
+        const long long *p = (j == job ? cur : jobs + j)->b_id;
+        return __ldg(p + (uint32_t)e);
+    }
+};
+
+__device__ __forceinline__ long long b_entry(uint32_t job, uint32_t gq)
+{
+    return (long long)(((unsigned long long)job << 32) | gq);
+}
+
 // Warp-aggregated append of this iteration's matches to the warp's buffer
-// (pb: address of idB; read here only for entries that overflow the buffer).
-__device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, long long ida, const long long *pb,
-                                       double dist, uint32_t job)
+// (gq: index of the matched B object in its segment).  Entries beyond the
+// buffer, which only the per-lane cursor path can produce, are written out
+// directly.
+template <bool DIST>
+__device__ __forceinline__ void emit_w(WBufT<DIST> &wb, const MatchOut &out, const IdSrc &ids, bool m, long long ida,
+                                       uint32_t gq, double dist, uint32_t job)
 {
     const unsigned act = __activemask();
     const unsigned bal = __ballot_sync(act, m);
@@ -395,9 +420,8 @@ __device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, lo
     base = __shfl_sync(bal, base, leader);
     const uint32_t slot = base + rank;
     if (slot < (uint32_t)kWarpBuf) {
-        wb.ab[slot] = make_longlong2(ida, (long long)pb);
-        wb.d[slot] = dist;
-        wb.job[slot] = job;
+        wb.ab[slot] = make_longlong2(ida, b_entry(job, gq));
+        if (DIST) wb.d[slot] = dist;
     }
     if (base + n <= (uint32_t)kWarpBuf) return;
     const uint32_t keep = base >= (uint32_t)kWarpBuf ? 0u : (uint32_t)kWarpBuf - base;
@@ -407,24 +431,27 @@ __device__ __forceinline__ void emit_w(WBuf &wb, const MatchOut &out, bool m, lo
     const int l2 = __ffs(over) - 1;
     unsigned long long g = 0;
     if ((int)lane == l2) g = atomicAdd(&out.counters[0], (unsigned long long)__popc(over));
-    const long long idb = __ldg(pb);
+    const long long idb = ids.id_of((unsigned long long)b_entry(job, gq));
     g = __shfl_sync(over, g, l2);
     g += (unsigned long long)__popc(over & lanemask_lt());
     if (g < out.cap) {
         reinterpret_cast<longlong2 *>(out.pairs)[g] = make_longlong2(ida, idb);
-        if (out.dist) out.dist[g] = dist;
+        if (DIST && out.dist) out.dist[g] = dist;
         if (out.job) out.job[g] = job;
     }
 }
 
-// Whole warp (converged): one atomicAdd, the idB loads issued under it, then a
-// coalesced copy (entry k by lane k).
-__device__ __forceinline__ void flush_w(WBuf &wb, const MatchOut &out)
+// Whole warp (converged): writes out the buffer's first min(count, 32)
+// entries -- one atomicAdd reserves their output slots, the idB loads are
+// issued under it, then entry k is stored by lane k (coalesced) -- and moves
+// the rest to the front.
+template <bool DIST>
+__device__ __forceinline__ void out_flush(WBufT<DIST> &wb, const MatchOut &out, const IdSrc &ids)
 {
-    static_assert(kWarpBuf == 32, "one buffer entry per lane");
     __syncwarp();
     const unsigned lane = threadIdx.x & 31;
-    const uint32_t n = wb.count < (uint32_t)kWarpBuf ? wb.count : (uint32_t)kWarpBuf;
+    const uint32_t held = min(wb.count, (uint32_t)kWarpBuf);
+    const uint32_t n = min(held, 32u);
     unsigned long long g = 0;
     if (lane == 0 && n) g = atomicAdd(&out.counters[0], (unsigned long long)n);
     longlong2 e = make_longlong2(0, 0);
@@ -432,18 +459,29 @@ __device__ __forceinline__ void flush_w(WBuf &wb, const MatchOut &out)
     uint32_t jb = 0;
     if (lane < n) {
         e = wb.ab[lane];
-        e.y = __ldg(reinterpret_cast<const long long *>(e.y));
-        if (out.dist) d = wb.d[lane];
-        if (out.job) jb = wb.job[lane];
+        jb = (uint32_t)((unsigned long long)e.y >> 32);
+        e.y = ids.id_of((unsigned long long)e.y);
+        if (DIST) d = wb.d[lane];
     }
-    g = __shfl_sync(0xffffffffu, g, 0);
-    if (lane < n && g + lane < out.cap) {
-        reinterpret_cast<longlong2 *>(out.pairs)[g + lane] = e;
-        if (out.dist) out.dist[g + lane] = d;
-        if (out.job) out.job[g + lane] = jb;
+    const uint32_t rest = held - n;
+    longlong2 e2 = make_longlong2(0, 0);
+    double d2 = 0;
+    if (lane < rest) {
+        e2 = wb.ab[32 + lane];
+        if (DIST) d2 = wb.d[32 + lane];
     }
     __syncwarp();
-    if (lane == 0) wb.count = 0;
+    if (lane < rest) {
+        wb.ab[lane] = e2;
+        if (DIST) wb.d[lane] = d2;
+    }
+    if (lane == 0) wb.count = rest;
+    g = __shfl_sync(0xffffffffu, g, 0) + lane;
+    if (lane < n && g < out.cap) {
+        reinterpret_cast<longlong2 *>(out.pairs)[g] = e;
+        if (DIST && out.dist) out.dist[g] = d;
+        if (out.job) out.job[g] = jb;
+    }
     __syncwarp();
 }
 
@@ -626,8 +664,8 @@ __device__ __forceinline__ uint32_t staged_global(const BView &V, int nseg, uint
 
 // All candidates of one A object against the view; emits matches.
 template <int VARIANT, bool COUNT_CAND, bool DIST>
-__device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BView &V, WBuf &wb, const MatchOut &out,
-                                            uint32_t jx, Counters &cn)
+__device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BView &V, WBufT<DIST> &wb,
+                                            const MatchOut &out, const IdSrc &ids, uint32_t jx, Counters &cn)
 {
     a.w = make_win(a.ra, a.alpha, J.raq_shift);
     Cursor c;
@@ -674,13 +712,13 @@ __device__ __forceinline__ void test_object(const JobDev &J, AObj &a, const BVie
                 m = c2 < J.sr_dist2;
             }
         }
-        const long long *pb = nullptr;
+        uint32_t gq = 0;
         double dist = 0;
         if (m) {
-            pb = &J.b_id[global_index(V, c.zb, q)];
+            gq = global_index(V, c.zb, q);
             if (DIST) dist = 2.0 * asin(sqrt(c2) * 0.5);
         }
-        emit_w(wb, out, m, a.id, pb, dist, jx);
+        emit_w<DIST>(wb, out, ids, m, a.id, gq, dist, jx);
     }
 }
 
@@ -1006,6 +1044,9 @@ static_assert(stage_aligned<64, false>() && stage_aligned<128, false>() && stage
                   stage_aligned<64, true>() && stage_aligned<128, true>() && stage_aligned<256, true>(),
               "bulk-copy destinations in a stage are 16-byte aligned");
 
+// Register caps: blocks of 256 objects two per SM -- registers are allocated
+// per scheduler partition, and 5 of a pair of blocks' 18 warps share one, so 96
+// a thread (5 x 96 x 32 <= 16K) -- and of 128 four.
 template <int TILE, int VARIANT, bool COUNT_CAND, bool DIST>
 __global__ void __launch_bounds__(TILE + 32, TILE <= 128 ? 4 : 2)
 pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans, uint32_t n_heavy,
@@ -1017,6 +1058,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
     constexpr int C = TILE / 32;   // consumer warps
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Stage *stages = reinterpret_cast<Stage *>(smem_raw);
+    using WBuf = WBufT<DIST>;
     WBuf *wbufs = reinterpret_cast<WBuf *>(stages + kStages);
     WList *wl = reinterpret_cast<WList *>(wbufs + C);
     uint64_t *full = reinterpret_cast<uint64_t *>(wl + C);
@@ -1239,6 +1281,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             Jp = &jobs[cur_job];
             K = load_scalars(*Jp);
         }
+        const IdSrc ids = {jobs, Jp, cur_job};
         const JobDev &J = *Jp;
         if (S.mode == PLAN_GLOBAL) {
             // band too large to stage: per-lane cursor over global memory
@@ -1268,7 +1311,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 V.band_lo = 0;
                 V.bins = J.b_bins;
                 V.bin_log2 = J.b_bin_log2;
-                test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
+                test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, ids, S.job, cn);
             }
         } else {
             BView V;
@@ -1317,7 +1360,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     a.full_ring = alpha >= 3.0;
                     a.id = S.a_id[S.id_skew + t];
                     a.gi = S.a_start + t;
-                        test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, S.job, cn);
+                        test_object<VARIANT, COUNT_CAND, DIST>(J, a, V, wb, out, ids, S.job, cn);
                 }
             } else {
                 // inclusive scan of candidate counts across the warp
@@ -1350,7 +1393,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                     const uint32_t own_start = __shfl_sync(0xffffffffu, start, own);
                     bool m = false;
                     long long ida = 0;
-                    const long long *pb = nullptr;
+                    uint32_t gq = 0xFFFFFFFFu;   // global index of the candidate, once needed
                     double dist = 0;
                     if (c < total) {
                         const int owner = own;
@@ -1367,7 +1410,6 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                         const double2 ra = S.a_radec[ta];
                         const double al = L.alpha[owner];
                         double c2 = 0;
-                        uint32_t gq = 0xFFFFFFFFu;   // global index of q, once needed
                         if (VARIANT == 0) {
                             const float4 fa = S.a_xyz[ta];
                             const float4 fb = S.b_xyz[q];
@@ -1420,25 +1462,25 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                         if (m) {
                             if (gq == 0xFFFFFFFFu) gq = staged_global(V, (int)S.nseg, q);
                             ida = S.a_id[S.id_skew + ta];
-                            pb = &J.b_id[gq];
                             if (DIST) dist = 2.0 * asin(sqrt(c2) * 0.5);
                         }
                     }
-                    emit_w(wb, out, m, ida, pb, dist, S.job);
+                    emit_w<DIST>(wb, out, ids, m, ida, gq, dist, S.job);
                     __syncwarp();
-                    if (wb.count >= (uint32_t)(kWarpBuf / 2)) flush_w(wb, out);
+                    if (wb.count >= 32u) out_flush<DIST>(wb, out, ids);
                 }
             }
         }
         __syncwarp();
         if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[s])) : "memory");
-        if (wb.count >= (uint32_t)(kWarpBuf / 2)) flush_w(wb, out);
+        if (wb.count >= 32u) out_flush<DIST>(wb, out, ids);
         if (++s == kStages) {
             s = 0;
             phase ^= 1u;
         }
     }
-    flush_w(wb, out);
+    const IdSrc ids = {jobs, Jp, cur_job};
+    while (min(wb.count, (uint32_t)kWarpBuf) > 0) out_flush<DIST>(wb, out, ids);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         cn.tested += __shfl_down_sync(0xffffffffu, cn.tested, o);
@@ -1454,20 +1496,27 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
     }
 }
 
-template <int TILE, bool RADEC>
+template <int TILE, bool RADEC, bool DIST>
 constexpr size_t smem_bytes()
 {
     using Stage = StageT<TILE, RADEC>;
-    return Stage::kStages * sizeof(Stage) + (TILE / 32) * (sizeof(WBuf) + sizeof(WList)) +
+    return Stage::kStages * sizeof(Stage) + (TILE / 32) * (sizeof(WBufT<DIST>) + sizeof(WList)) +
            2 * Stage::kStages * sizeof(uint64_t);
 }
+
+// Blocks of 256 objects run two per SM, blocks of 128 of the kernels without
+// distances four (228 KB of shared memory per SM, 1 KB of it reserved per block).
+static_assert(2 * (smem_bytes<256, true, true>() + 1024) <= 228 * 1024 &&
+                  2 * (smem_bytes<256, false, true>() + 1024) <= 228 * 1024 &&
+                  4 * (smem_bytes<128, false, false>() + 1024) <= 228 * 1024,
+              "pair-kernel blocks per SM");
 
 template <int TILE, int VARIANT, bool CC, bool DIST>
 cudaError_t launch_t(const LaunchCfg &L, const JobDev *jobs, const TilePlan *plans, uint32_t n_heavy,
                      uint32_t n_normal, const MatchOut &out, cudaStream_t st)
 {
     auto k = pair_kernel<TILE, VARIANT, CC, DIST>;
-    const size_t smem = smem_bytes<TILE, VARIANT == 1>();
+    const size_t smem = smem_bytes<TILE, VARIANT == 1, DIST>();
     static bool attr = false;   // per instantiation
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
