@@ -337,13 +337,16 @@ def test_crossmatch_streams_a_in_chunks(ctx, fixtures, monkeypatch):
         p, d = sp(p, d)
         assert np.array_equal(p, po) and np.max(np.abs(d - do), initial=0) <= DIST_TOL
     # explicit schedules: the largest chunk not the first (the staging slots take
-    # the largest), a chunk of one object, an empty chunk
-    for w in ("1,3,1", "9997,1,2", "1,0.00001,1"):
+    # the largest), a chunk of one object, an empty chunk; rings of 2, 3 and 5 slots
+    for w, slots in (("1,3,1", "2"), ("9997,1,2", "3"), ("1,0.00001,1", "2"), ("5,1,4,2,3,1,1", "3"),
+                     ("1,1,1,1,1", "5")):
         monkeypatch.setenv("XMATCH_CHUNK_WEIGHTS", w)
+        monkeypatch.setenv("XMATCH_CHUNK_SLOTS", slots)
         p, d, st = ctx.crossmatch(a, a2, r, out=(P, D))
         p, d = sp(p, d)
         assert np.array_equal(p, po) and np.max(np.abs(d - do), initial=0) <= DIST_TOL
     monkeypatch.delenv("XMATCH_CHUNK_WEIGHTS")
+    monkeypatch.delenv("XMATCH_CHUNK_SLOTS")
     # room for fewer than all: the whole match reruns into device buffers, the count is reported
     import xmatch_b200 as xm
     with pytest.raises(xm.XmatchError) as e:

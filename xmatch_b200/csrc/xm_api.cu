@@ -985,12 +985,23 @@ namespace {
 // has landed: n chunks of relative sizes n + 1, n, ..., 2, n = nA / 10M (5 at
 // 50M: 48.9 ms at 50M x 50M against 50.1 ms for 4 equal chunks and 59 ms for
 // one).  Environment XMATCH_CHUNK_OBJS sets the objects per chunk that fix n,
-// XMATCH_CHUNK_WEIGHTS (comma-separated relative sizes) the whole schedule.
+// XMATCH_CHUNK_WEIGHTS (comma-separated relative sizes, at most kMaxChunks) the
+// whole schedule.
+constexpr uint64_t kMaxChunks = 16;   // = the context's staging-slot events
+
 uint64_t chunk_objs()
 {
     const char *e = std::getenv("XMATCH_CHUNK_OBJS");
     const unsigned long long v = e ? std::strtoull(e, nullptr, 10) : 0ull;
     return v ? (uint64_t)v : 10000000ull;
+}
+
+// Staging slots of A's chunks (environment XMATCH_CHUNK_SLOTS, at least 2).
+uint64_t chunk_slots()
+{
+    const char *e = std::getenv("XMATCH_CHUNK_SLOTS");
+    const unsigned long long v = e ? std::strtoull(e, nullptr, 10) : 0ull;
+    return v ? std::max<uint64_t>(2, std::min<uint64_t>(kMaxChunks, v)) : 2;
 }
 
 // Chunk boundaries of A: bounds[c] .. bounds[c + 1] is chunk c.
@@ -1006,6 +1017,7 @@ std::vector<uint64_t> chunk_bounds(uint64_t nA, uint64_t n_chunks)
             p = *end == ',' ? end + 1 : end;
         }
     }
+    if (w.size() > kMaxChunks) w.clear();
     if (w.empty()) {
         for (uint64_t c = 0; c < n_chunks; ++c) w.push_back((double)(n_chunks + 1 - c));
     }
@@ -1069,28 +1081,30 @@ extern "C" xm_status xm_crossmatch(xm_ctx *ctx, const xm_obj *A, uint64_t nA, co
         direct.capacity = out->capacity;
     }
     const bool streamed = direct.pairs && (!want_dist || direct.dist);
-    const uint64_t n_even = streamed ? std::max<uint64_t>(1, std::min<uint64_t>(16, nA / chunk_objs())) : 1;
+    const uint64_t n_even = streamed ? std::max<uint64_t>(1, std::min<uint64_t>(kMaxChunks, nA / chunk_objs())) : 1;
     const std::vector<uint64_t> bounds = n_even > 1 ? chunk_bounds(nA, n_even) : std::vector<uint64_t>{0, nA};
     const uint64_t n_chunks = bounds.size() - 1;
     uint64_t chunk = 0;   // the largest chunk: the size of a staging slot
     for (uint64_t c = 0; c < n_chunks; ++c) chunk = std::max(chunk, bounds[c + 1] - bounds[c]);
-    // A chunks land in two slots of the staging buffer, copied on the second stream
-    XM_TRY(grow(ctx, &ctx->stage, &ctx->stage_bytes, 2 * std::max<uint64_t>(chunk, 1) * sizeof(xm_obj)));
-    xm_obj *slot[2] = {(xm_obj *)ctx->stage, (xm_obj *)ctx->stage + std::max<uint64_t>(chunk, 1)};
+    // A's chunks land in a ring of staging slots, copied on the second stream: chunk
+    // c + n_slots is copied once chunk c's build has read its slot
+    const uint64_t n_slots = std::min<uint64_t>(n_chunks, chunk_slots());
+    const uint64_t slot_objs = std::max<uint64_t>(chunk, 1);
+    XM_TRY(grow(ctx, &ctx->stage, &ctx->stage_bytes, n_slots * slot_objs * sizeof(xm_obj)));
+    auto slot = [&](uint64_t c) { return (xm_obj *)ctx->stage + (c % n_slots) * slot_objs; };
     cudaEvent_t *landed = ctx->ev_slot;   // recorded only here
     auto copy_chunk = [&](uint64_t c) -> xm_status {
         const uint64_t first = bounds[c], n = bounds[c + 1] - bounds[c];
-        if (n) XM_CUDA(ctx, cudaMemcpyAsync(slot[c & 1], A + first, n * sizeof(xm_obj), cudaMemcpyHostToDevice, s2));
-        XM_CUDA(ctx, cudaEventRecord(landed[c & 1], s2));
+        if (n) XM_CUDA(ctx, cudaMemcpyAsync(slot(c), A + first, n * sizeof(xm_obj), cudaMemcpyHostToDevice, s2));
+        XM_CUDA(ctx, cudaEventRecord(landed[c % n_slots], s2));
         return XM_OK;
     };
     xm_segment *sb = nullptr, *sa = nullptr;
     xm_status rc = new_segment(ctx, 1, zh_deg, &sb);
     if (rc == XM_OK && streamed) {
-        // A's first two chunks follow B on the link
+        // A's first n_slots chunks follow B on the link
         if (cudaStreamWaitEvent(s2, ctx->ev_b2, 0) != cudaSuccess) rc = XM_ERR_CUDA;
-        if (rc == XM_OK) rc = copy_chunk(0);
-        if (rc == XM_OK && n_chunks > 1) rc = copy_chunk(1);
+        for (uint64_t c = 0; rc == XM_OK && c < n_slots; ++c) rc = copy_chunk(c);
     }
     if (rc == XM_OK) rc = xm_build_impl(sb, (const xm_obj *)ctx->stage2, nB, stats);
     if (rc == XM_OK && stats) {
@@ -1106,12 +1120,12 @@ extern "C" xm_status xm_crossmatch(xm_ctx *ctx, const xm_obj *A, uint64_t nA, co
         rc = new_segment(ctx, 0, zh_deg, &sa);
         for (uint64_t c = 0; rc == XM_OK && c < n_chunks; ++c) {
             const uint64_t n = bounds[c + 1] - bounds[c];
-            if (cudaStreamWaitEvent(st, landed[c & 1], 0) != cudaSuccess) {
+            if (cudaStreamWaitEvent(st, landed[c % n_slots], 0) != cudaSuccess) {
                 rc = XM_ERR_CUDA;
                 break;
             }
-            rc = xm_build_impl(sa, slot[c & 1], n, stats);   // returns with the slot read (stream synchronised)
-            if (rc == XM_OK && c + 2 < n_chunks) rc = copy_chunk(c + 2);
+            rc = xm_build_impl(sa, slot(c), n, stats);   // returns with the slot read (stream synchronised)
+            if (rc == XM_OK && c + n_slots < n_chunks) rc = copy_chunk(c + n_slots);
             if (rc != XM_OK) break;
             xm_job job = {sa, sb, sr_deg};
             xm_pairs dc = direct;

@@ -78,7 +78,7 @@ struct xm_ctx {
     size_t stage2_bytes = 0;
     cudaStream_t stream2 = nullptr;   // copies that overlap work on stream
     cudaEvent_t ev_b2 = nullptr;
-    cudaEvent_t ev_slot[2] = {nullptr, nullptr};   // xm_crossmatch: a chunk of A has landed in a staging slot
+    cudaEvent_t ev_slot[16] = {};   // xm_crossmatch: a chunk of A has landed in a staging slot
     size_t build_tmp_bytes = 0;
     cudaGraphExec_t graph_exec = nullptr;   // the pair-kernel launch sequence (see xm_run_jobs)
     uint64_t graph_launches = 0;
