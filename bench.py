@@ -365,8 +365,8 @@ def run_ours(args):
     # catalogs cut to dec 30..60 deg (same objects per zone; 8,919,127 A objects), scaled by the objects a
     # launch processes
     band_a = 8_919_127
-    traffic_per_obj = {"pair_kernel": (579.86e6 + 91.85e6) / band_a, "zb_scatter": (214.17e6 + 235.99e6) / band_a,
-                       "zb_zone_sort": (300.30e6 + 310.54e6) / band_a, "pair_plan": 3.01e6 / 4_397_838}
+    traffic_per_obj = {"pair_kernel": (579.86e6 + 91.85e6) / band_a, "zb_scatter": (214.11e6 + 237.19e6) / band_a,
+                       "zb_zone_sort": (313.78e6 + 312.82e6) / band_a, "pair_plan": 3.01e6 / 4_397_838}
     units = {"pair_kernel": kept_a, "pair_plan": kept_a, "zb_scatter": nc, "zb_zone_sort": nc}
     for k in stages:
         if k in traffic_per_obj:
