@@ -1013,16 +1013,20 @@ std::vector<uint64_t> chunk_bounds(uint64_t nA, uint64_t n_chunks)
             char *end = nullptr;
             const double v = std::strtod(p, &end);
             if (end == p) break;
-            if (v > 0) w.push_back(v);
+            if (v > 0 && std::isfinite(v)) w.push_back(v);
             p = *end == ',' ? end + 1 : end;
         }
     }
-    if (w.size() > kMaxChunks) w.clear();
-    if (w.empty()) {
-        for (uint64_t c = 0; c < n_chunks; ++c) w.push_back((double)(n_chunks + 1 - c));
-    }
     double sum = 0;
     for (double v : w) sum += v;
+    if (w.size() > kMaxChunks || !std::isfinite(sum)) w.clear();
+    if (w.empty()) {
+        sum = 0;
+        for (uint64_t c = 0; c < n_chunks; ++c) {
+            w.push_back((double)(n_chunks + 1 - c));
+            sum += w.back();
+        }
+    }
     std::vector<uint64_t> b(1, 0);
     double acc = 0;
     for (size_t c = 0; c < w.size(); ++c) {
