@@ -124,6 +124,36 @@ __device__ __forceinline__ Win make_win(double ra, double alpha, int shift)
     return w;
 }
 
+// The same windows in quantised-ra units from A's own quantised ra (xyz.w) and
+// alpha: any B within alpha of A in ra (in one of the three branches) has a
+// quantised ra within alpha * 2^26 / pi + 3 of A's -- 1 for the floor of each,
+// 1 for the rounding of each product in raq32 -- so these windows hold every
+// object of the FP64 ones, and the predicate decides.  Used with alpha < 3
+// (pi - 3 apart, the three windows are disjoint); full-ring zones enumerate
+// the whole zone instead.
+constexpr double kRaqPerRad = XM_RAQ_SCALE / 32.0;   // 2^26 / pi: units of the 27-bit quantised ra per radian
+
+__device__ __forceinline__ Win make_win_q(uint32_t ra_q, double alpha)
+{
+    constexpr uint32_t kTurn = 1u << 27;
+    const double aqd = ceil(__dmul_rn(alpha, kRaqPerRad)) + 3.0;
+    const uint32_t aq = aqd < (double)kTurn ? (uint32_t)aqd : kTurn;
+    Win w;
+    w.lo = ra_q > aq ? ra_q - aq : 0u;
+    w.hi = min(ra_q + aq, kTurn - 1u);   // ra_q, aq <= 2^27: no overflow
+    w.lo2 = w.lo3 = 0xFFFFFFFFu;
+    w.hi2 = w.hi3 = 0u;
+    if (ra_q + aq >= kTurn) {            // branch 2: B near 0
+        w.lo2 = 0u;
+        w.hi2 = ra_q + aq - kTurn;
+    }
+    if (ra_q < aq) {                     // branch 3: B near 2 pi
+        w.lo3 = ra_q + kTurn - aq;
+        w.hi3 = kTurn - 1u;
+    }
+    return w;
+}
+
 // FP64 chord^2 of two positions from their unit vectors, computed as the zone
 // builder computes them (the same bits).
 __device__ __forceinline__ double chord2_radec_inl(double ra1, double dec1, double ra2, double dec2)
@@ -1053,6 +1083,9 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             uint32_t n_normal, uint32_t chunk, MatchOut out)
 {
     constexpr bool RADEC = VARIANT == 1;
+    // A's FP64 ra/dec staged only for the kernels that read them for every
+    // candidate (plain FP64, candidate counting, distances)
+    constexpr bool A_RADEC = RADEC || COUNT_CAND || DIST;
     using Stage = StageT<TILE, RADEC>;
     constexpr int kStages = Stage::kStages;
     constexpr int C = TILE / 32;   // consumer warps
@@ -1129,7 +1162,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 const uint32_t a_even = a_start & ~1u;
                 S.id_skew = a_start - a_even;
                 const uint32_t id_cnt = (a_start + a_len - a_even + 1) & ~1u;
-                uint32_t bytes = a_len * 32u + id_cnt * 8u;
+                uint32_t bytes = a_len * (A_RADEC ? 32u : 16u) + id_cnt * 8u;
                 // alpha of [zf, zl] and A offsets of [zf, zl + 1], rounded out to 16-byte copies
                 // (alpha tables carry 2 spare entries, zone offsets 8)
                 const uint32_t ae = (uint32_t)(zf - alpha_z0), ae_al = ae & ~1u;
@@ -1165,7 +1198,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 }
                 fence_proxy_async();
                 mbar_expect_tx(&full[s], bytes);
-                bulk_g2s(S.a_radec, a_radec + a_start, a_len * 16u, &full[s]);
+                if (A_RADEC) bulk_g2s(S.a_radec, a_radec + a_start, a_len * 16u, &full[s]);
                 bulk_g2s(S.a_xyz, a_xyz + a_start, a_len * 16u, &full[s]);
                 bulk_g2s(S.a_id, a_id + a_even, id_cnt * 8u, &full[s]);
                 bulk_g2s(S.alpha_s, alpha + ae_al, acnt * 8u, &full[s]);
@@ -1288,7 +1321,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             if (t < S.a_len) {
                 AObj a;
                 const float4 fa = S.a_xyz[t];
-                const double2 ra = S.a_radec[t];
+                const double2 ra = A_RADEC ? S.a_radec[t] : __ldg(&J.a_radec[S.a_start + t]);
                 a.ra = ra.x;
                 a.dec = ra.y;
                 a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
@@ -1329,11 +1362,8 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
             // ---- phase 1: each lane's candidate ranges ----
             WList &L = wl[warp - 1];
             int n = 0, nr = 0, za = 0;
-            double ra_a = 0, dec_a = 0, alpha = 0;
+            double alpha = 0;
             if (t < S.a_len) {
-                const double2 rd = S.a_radec[t];
-                ra_a = rd.x;
-                dec_a = rd.y;
                 za = a_zone_s(S, S.a_start + t);
                 if (za < 0) {
                     atomicExch(&out.counters[7], 1ull);
@@ -1342,7 +1372,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 } else {
                     alpha = S.alpha_s[S.alpha_skew + (za - S.zf)];
                 }
-                const Win wn = make_win(ra_a, alpha, K.raq_shift);
+                const Win wn = make_win_q(__float_as_uint(S.a_xyz[t].w), alpha);
                 n = lane_ranges(V, K, wn, alpha >= 3.0, za, L.r[lane], nr);
             }
             L.alpha[lane] = alpha;
@@ -1352,8 +1382,9 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                 if (t < S.a_len) {
                     AObj a;
                     const float4 fa = S.a_xyz[t];
-                    a.ra = ra_a;
-                    a.dec = dec_a;
+                    const double2 rd = A_RADEC ? S.a_radec[t] : __ldg(&J.a_radec[S.a_start + t]);
+                    a.ra = rd.x;
+                    a.dec = rd.y;
                     a.fx = fa.x; a.fy = fa.y; a.fz = fa.z;
                     a.zone = za;
                     a.alpha = alpha;
@@ -1407,7 +1438,10 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                         const uint32_t q = (rr & 0xFFFFu) + k;
                         const uint32_t ta = (warp - 1) * 32u + (uint32_t)owner;
                         cn.tested++;
-                        const double2 ra = S.a_radec[ta];
+                        // A's FP64 ra/dec: staged for the kernels that cut or measure every
+                        // pair, else read for the few pairs that need them
+                        double2 ra = make_double2(0.0, 0.0);
+                        if (A_RADEC) ra = S.a_radec[ta];
                         const double al = L.alpha[owner];
                         double c2 = 0;
                         if (VARIANT == 0) {
@@ -1433,7 +1467,10 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                                     if (gq == 0xFFFFFFFFu) gq = staged_global(V, (int)S.nseg, q);
                                     rb = __ldg(&J.b_radec[gq]);
                                 }
-                                if (cut) pass = cuts_k(K, ra.x, ra.y, al, rb);
+                                if (cut) {
+                                    if (!A_RADEC) ra = __ldg(&J.a_radec[S.a_start + ta]);
+                                    pass = cuts_k(K, ra.x, ra.y, al, rb);
+                                }
                                 if (pass) {
                                     m = true;
                                     if (band || DIST) {
