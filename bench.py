@@ -344,15 +344,17 @@ def run_ours(args):
     kept_a, kept_b = len(sa), len(sb)
     n_zones = int(np.ceil(180 / zh))
     nc = (n + nb) // 2   # mean catalog size (the zb_* stages are per catalog)
+    a_radec = args.dist or args.variant == "plain64"   # kernels that stage A's FP64 ra/dec
     alg_bytes = {   # algorithmic bytes per launch (per catalog for the zb_* stages)
         "zb_count": 24 * nc,                       # records in
         "zb_offsets": 16 * n_zones,                # counts in, offsets out, cursors
         "zb_scatter": (24 + 32) * nc,              # records in, 32-byte bucket records out
         "zb_zone_sort": (32 + 40) * nc,            # bucket records in; id, radec, xyz out
         "pair_plan": 64 * int(np.ceil(len(sa) / 128)),   # one 64-byte plan per tile
-        # A once (id, radec, FP32 xyz), B's FP32 xyz once, per match B's id and the pair out; with
-        # distances also the distance out and B's ra/dec in (the FP64 vectors are recomputed)
-        "pair_kernel": 40 * kept_a + 16 * kept_b + (24 + 8 + 16 if args.dist else 24) * n_match,
+        # A once (id and FP32 xyz; its FP64 ra/dec too with distances or the plain-FP64 kernel), B's FP32
+        # xyz once, per match B's id and the pair out; with distances also the distance out and B's ra/dec
+        # in (the FP64 vectors are recomputed)
+        "pair_kernel": (40 if a_radec else 24) * kept_a + 16 * kept_b + (24 + 8 + 16 if args.dist else 24) * n_match,
     }
     peaks, peak_kind = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
@@ -365,7 +367,7 @@ def run_ours(args):
     # catalogs cut to dec 30..60 deg (same objects per zone; 8,919,127 A objects), scaled by the objects a
     # launch processes
     band_a = 8_919_127
-    traffic_per_obj = {"pair_kernel": (579.86e6 + 91.85e6) / band_a, "zb_scatter": (214.11e6 + 237.19e6) / band_a,
+    traffic_per_obj = {"pair_kernel": (437.64e6 + 87.11e6) / band_a, "zb_scatter": (214.11e6 + 237.19e6) / band_a,
                        "zb_zone_sort": (313.78e6 + 312.82e6) / band_a, "pair_plan": 3.01e6 / 4_397_838}
     units = {"pair_kernel": kept_a, "pair_plan": kept_a, "zb_scatter": nc, "zb_zone_sort": nc}
     for k in stages:
@@ -376,9 +378,11 @@ def run_ours(args):
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per object on a dec-band cut of "
                                   "the same catalogs, times the objects of this launch",
                 "peak_source": peak_kind}
-    # per catalog: records read (24) and the sorted SoA written (40); the pair kernel: A read once (40), B's
-    # FP32 vectors read once (16), per match the record out (16 or 24) and B's id (8)
-    pipeline_bytes = (24 + 40) * (n + nb) + 40 * kept_a + 16 * kept_b + (32 if args.dist else 24) * n_match
+    # per catalog: records read (24) and the sorted SoA written (40); the pair kernel: A read once (24, or
+    # 40 with its FP64 ra/dec), B's FP32 vectors read once (16), per match the record out (16 or 24) and
+    # B's id (8)
+    pipeline_bytes = ((24 + 40) * (n + nb) + (40 if a_radec else 24) * kept_a + 16 * kept_b
+                      + (32 if args.dist else 24) * n_match)
     pipeline = {"alg_bytes": pipeline_bytes, "GB/s": pipeline_bytes / (ms * 1e-3) / 1e9,
                 "frac": pipeline_bytes / (ms * 1e-3) / 1e9 / hbm}
     value = whole_job_rate(world, n_cand, ms)
