@@ -11,10 +11,10 @@ from oracle import OBJ_DTYPE
 
 ARCSEC = 1.0 / 3600.0
 
-# Match counts computed independently while surveying the reference
-# (numpy restatement + brute-force all-pairs FP64 chord test), self-pairs
-# included, zh = r.
-SURVEY_COUNTS = {
+# Match counts of the reference's two fixture catalogs computed independently
+# of the oracle (a numpy restatement and a brute-force all-pairs FP64 chord
+# test), self-pairs included, zh = r.
+KNOWN_COUNTS = {
     ("test_x_test", 1): 10004, ("test_x_test", 5): 10980, ("test_x_test", 30): 41166,
     ("test2_x_test", 1): 1002, ("test2_x_test", 5): 1082, ("test2_x_test", 30): 4777,
     ("test2_x_test2", 1): 1002, ("test2_x_test2", 5): 1074, ("test2_x_test2", 30): 2748,
@@ -48,13 +48,13 @@ def brute_force(A, B, r_deg):
     return np.concatenate(out), near
 
 
-@pytest.mark.parametrize("name,r", sorted(SURVEY_COUNTS))
+@pytest.mark.parametrize("name,r", sorted(KNOWN_COUNTS))
 def test_known_counts_all_modes(fixtures, name, r):
     a, b = _cases(fixtures)[name]
     res = []
     for mode in (oracle.MODE_ALLPAIRS, oracle.MODE_ALLPAIRS_SINCOS, oracle.MODE_WINDOWED):
         p, d, st = oracle.xmatch(a, b, r * ARCSEC, mode=mode, nthreads=4)
-        assert len(p) == SURVEY_COUNTS[(name, r)]
+        assert len(p) == KNOWN_COUNTS[(name, r)]
         res.append((sorted_pairs(p, d), st.n_cand))
     for k in (1, 2):
         assert np.array_equal(res[0][0][0], res[k][0][0])
