@@ -515,7 +515,9 @@ __device__ __forceinline__ void out_flush(WBufT<DIST> &wb, const MatchOut &out, 
     __syncwarp();
 }
 
-// Per-tile job scalars kept in registers.
+// Per-tile job scalars kept in registers.  The FP32-filter kernels read the
+// FP64 radius and chord threshold from the job entry for the few pairs that
+// need them (inside the margin band, full-ring zones) instead of holding them.
 struct JobScalars {
     double sr_rad, sr_dist2;
     float thr_hi, thr_lo;
@@ -536,9 +538,9 @@ __device__ __forceinline__ JobScalars load_scalars(const JobDev &J)
     return k;
 }
 
-__device__ __forceinline__ bool cuts_k(const JobScalars &K, double ra_a, double dec_a, double alpha, double2 rb)
+__device__ __forceinline__ bool cuts_k(double sr_rad, double ra_a, double dec_a, double alpha, double2 rb)
 {
-    if (!(fabs(__dsub_rn(dec_a, rb.y)) < K.sr_rad)) return false;
+    if (!(fabs(__dsub_rn(dec_a, rb.y)) < sr_rad)) return false;
     const double d = __dsub_rn(ra_a, rb.x);
     return fabs(d) < alpha || fabs(__dsub_rn(d, XM_TWO_PI)) < alpha || fabs(__dadd_rn(d, XM_TWO_PI)) < alpha;
 }
@@ -1451,7 +1453,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                             const float c32 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                             if (COUNT_CAND) {
                                 gq = staged_global(V, (int)S.nseg, q);
-                                cn.cand += cuts_k(K, ra.x, ra.y, al, __ldg(&J.b_radec[gq])) ? 1ull : 0ull;
+                                cn.cand += cuts_k(J.sr_rad, ra.x, ra.y, al, __ldg(&J.b_radec[gq])) ? 1ull : 0ull;
                             }
                             if (!(c32 > K.thr_hi)) {
                                 // below thr_lo the FP64 chord is under the threshold and, in a zone
@@ -1469,7 +1471,7 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                                 }
                                 if (cut) {
                                     if (!A_RADEC) ra = __ldg(&J.a_radec[S.a_start + ta]);
-                                    pass = cuts_k(K, ra.x, ra.y, al, rb);
+                                    pass = cuts_k(J.sr_rad, ra.x, ra.y, al, rb);
                                 }
                                 if (pass) {
                                     m = true;
@@ -1479,14 +1481,14 @@ pair_kernel(const JobDev *__restrict__ jobs, const TilePlan *__restrict__ plans,
                                         c2 = chord2_radec<DIST>(ra.x, ra.y, rb.x, rb.y);
                                         if (band) {
                                             cn.exact++;
-                                            m = c2 < K.sr_dist2;
+                                            m = c2 < J.sr_dist2;
                                         }
                                     }
                                 }
                             }
                         } else {
                             const double2 rb = S.b_radec[q];
-                            if (cuts_k(K, ra.x, ra.y, al, rb)) {
+                            if (cuts_k(K.sr_rad, ra.x, ra.y, al, rb)) {
                                 cn.cand++;
                                 cn.exact++;
                                 double x1, y1, z1, x2, y2, z2;
