@@ -137,7 +137,8 @@ __device__ __forceinline__ Win make_win_q(uint32_t ra_q, double alpha)
 {
     constexpr uint32_t kTurn = 1u << 27;
     const double aqd = ceil(__dmul_rn(alpha, kRaqPerRad)) + 3.0;
-    const uint32_t aq = aqd < (double)kTurn ? (uint32_t)aqd : kTurn;
+    // alpha < 0 marks a tile whose zone offsets disagree (already reported as an error)
+    const uint32_t aq = !(aqd >= 0.0) ? 0u : aqd < (double)kTurn ? (uint32_t)aqd : kTurn;
     Win w;
     w.lo = ra_q > aq ? ra_q - aq : 0u;
     w.hi = min(ra_q + aq, kTurn - 1u);   // ra_q, aq <= 2^27: no overflow
